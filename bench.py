@@ -1,0 +1,364 @@
+"""Benchmark of the PME reciprocal path: evals/s on one B200 (or N independent replicas).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                    [--workload water8k_64_p4|water1k_32|water8k_64_p6|water336k_216_p6]
+
+One step = one full reciprocal evaluation (spread, R2C, solve with energy+virial, C2R, gather,
+self energy) of the workload.  The default workload is 8,000 TIP3P-geometry waters (24,000
+atoms) in a 62.1 A cube, 64^3 grid, spline order 4, kappa 0.32 (seeded synthetic data).
+
+value: device-timed evals/s with inputs resident in HBM, L2 flushed (256 MiB write) before every
+step outside the per-step CUDA-event pair.  e2e: the same through the C ABI with host buffers:
+pinned xyzq H2D, evaluation, forces + energy/virial D2H, all inside the timed region.
+roofline: the dominant stage of the staged C-ABI calls, timed with CUDA events on the
+operator's stream, algorithmic bytes per launch against the measured HBM copy bandwidth.
+--impl reference: the CPU oracle (multithreaded FP64 restatement of the reference algorithm;
+the reference itself has no CPU path and its GPU code does not build for sm_100a unmodified).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "PME recip evals/s at 24k atoms/64^3; batched evals/s + p50/p99 latency, same GPU"
+UNIT = "evals/s"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="water8k_64_p4")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0,
+                    help="time budget of the cpu_baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def make_workload(name: str, rank: int = 0):
+    from gpu_recip_b200 import systems as S
+    if name == "water8k_64_p4":
+        s = S.config_production(4, seed=2 + 1000 * rank)
+    elif name == "water8k_64_p6":
+        s = S.config_production(6, seed=2 + 1000 * rank)
+    elif name == "water1k_32":
+        s = S.config_small(seed=1 + 1000 * rank)
+    elif name == "water336k_216_p6":
+        s = S.config_large(seed=3 + 1000 * rank)
+    else:
+        raise SystemExit(f"unknown workload {name}")
+    return s
+
+
+def workload_config(s, extra=None):
+    cfg = {"workload": f"{s.name}: {s.natom} atoms TIP3P-geometry water, box {s.box[0]:.2f} A, "
+                       f"grid {s.nfft[0]}x{s.nfft[1]}x{s.nfft[2]}, order {s.order}, kappa {s.kappa}",
+           "natom": s.natom, "nfft": list(s.nfft), "order": s.order, "kappa": s.kappa,
+           "alg_bytes_per_eval": s.alg_bytes(), "l2": "flushed (256 MiB write) before every step"}
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.tmp = tempfile.NamedTemporaryFile(mode="w+", suffix=".csv", delete=False)
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.gpu), "-lms", "200"], stdout=self.tmp,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        self.tmp.flush()
+        rows = []
+        try:
+            with open(self.tmp.name) as fh:
+                for line in fh:
+                    parts = [p.strip() for p in line.split(",")]
+                    if len(parts) >= 9:
+                        rows.append(parts)
+        finally:
+            try:
+                os.unlink(self.tmp.name)
+            except OSError:
+                pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_oracle_rate(s, seconds: float, nthreads: int = 0):
+    from oracle import oracle as O
+    O.build()
+    x = s.xyzq.astype(np.float64)
+    O.evaluate(x, s.recip3, s.nfft, s.order, s.kappa, nthreads)  # warm-up
+    n = 0
+    t0 = time.perf_counter()
+    while True:
+        O.evaluate(x, s.recip3, s.nfft, s.order, s.kappa, nthreads)
+        n += 1
+        dt = time.perf_counter() - t0
+        if dt >= seconds or n >= 1000:
+            break
+    cores = nthreads if nthreads > 0 else O.hardware_threads()
+    return n / dt, n, dt, cores
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    s = make_workload(args.workload)
+    from oracle import oracle as O
+    O.build()
+    x = s.xyzq.astype(np.float64)
+    for _ in range(max(1, args.warmup)):
+        O.evaluate(x, s.recip3, s.nfft, s.order, s.kappa)
+    # each step is one full evaluation, capped so the run stays within a few minutes
+    steps = args.steps
+    t0 = time.perf_counter()
+    done = 0
+    budget = 150.0
+    while done < steps:
+        O.evaluate(x, s.recip3, s.nfft, s.order, s.kappa)
+        done += 1
+        if time.perf_counter() - t0 > budget:
+            break
+    dt = time.perf_counter() - t0
+    rate = done / dt
+    cores = O.hardware_threads()
+    sample = f"{done} full FP64 evaluations of the workload on {cores} host threads"
+    line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": done, "warmup": args.warmup, "ms_per_step": 1000.0 * dt / done,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded TIP3P-geometry water)",
+            "config": workload_config(s, {"parallelism": "cpu threads", "l2": "n/a (CPU)"}),
+            "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "reference has no CPU implementation of the path; this is the oracle port of its algorithm"}
+    print(json.dumps(line), flush=True)
+
+
+def run_b200(args):
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.device("cuda", torch.cuda.current_device())
+
+    from gpu_recip_b200 import CudaPMERecip, force_stride, load_library
+    from gpu_recip_b200 import build as B
+    if rank == 0 or world == 1:
+        B.build()
+    if world > 1:
+        dist.barrier()
+    load_library()
+
+    s = make_workload(args.workload, rank)
+    n = s.natom
+    stride = force_stride(n)
+    stream = torch.cuda.Stream(device=dev)
+    pme = CudaPMERecip(*s.nfft, s.order, stream=stream)
+    inv_box = [1.0 / b for b in s.box]
+    recip = [inv_box[0], 0, 0, 0, inv_box[1], 0, 0, 0, inv_box[2]]
+    x_dev = torch.from_numpy(s.xyzq).to(dev)
+    f_dev = torch.zeros(3 * stride, dtype=torch.float32, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def one_eval():
+        pme.energy_virial.clear()
+        pme.eval_ortho(inv_box, x_dev, n, s.kappa, True, True, f_dev, stride)
+
+    kernels_per_eval = 8   # spread, x_r2c, y fwd, z fwd+solve+inv, y inv, x_c2r, gather, self
+
+    with torch.cuda.stream(stream):
+        for _ in range(max(3, args.warmup)):
+            flush.fill_(0.0)
+            one_eval()
+    stream.synchronize()
+
+    K = args.steps
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    clocks = ClockSampler(dev.index)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with clocks:
+        with torch.cuda.stream(stream):
+            for i in range(K):
+                flush.fill_(float(i & 7))
+                starts[i].record(stream)
+                one_eval()
+                ends[i].record(stream)
+        stream.synchronize()
+    torch.cuda.synchronize()
+    per = np.array([starts[i].elapsed_time(ends[i]) for i in range(K)])  # ms
+    total_ms = float(per.sum())
+    if world > 1:
+        t = torch.tensor([total_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        dist.barrier()
+    value = world * K / (total_ms / 1000.0)
+
+    # ---- e2e through the C ABI with host buffers -------------------------------------------------
+    x_host = torch.from_numpy(s.xyzq).pin_memory()
+    f_host = torch.empty(3 * stride, dtype=torch.float32).pin_memory()
+    ev_host = torch.empty(11, dtype=torch.float64).pin_memory()
+    Ke = max(10, K // 4)
+    e_starts = [torch.cuda.Event(enable_timing=True) for _ in range(Ke)]
+    e_ends = [torch.cuda.Event(enable_timing=True) for _ in range(Ke)]
+    x_in = torch.empty_like(x_dev)
+    with torch.cuda.stream(stream):
+        for i in range(Ke + 3):
+            flush.fill_(0.0)
+            if i >= 3:
+                e_starts[i - 3].record(stream)
+            x_in.copy_(x_host, non_blocking=True)
+            pme.energy_virial.clear()
+            pme.eval_ortho(inv_box, x_in, n, s.kappa, True, True, f_dev, stride)
+            f_host.copy_(f_dev, non_blocking=True)
+            pme.energy_virial.copy_async(ev_host)
+            if i >= 3:
+                e_ends[i - 3].record(stream)
+    stream.synchronize()
+    e_total = float(sum(e_starts[i].elapsed_time(e_ends[i]) for i in range(Ke)))
+    if world > 1:
+        t = torch.tensor([e_total], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e_total = float(t.item())
+    e2e_value = world * Ke / (e_total / 1000.0)
+
+    # ---- per-stage timing (staged C-ABI calls) for the roofline -------------------------------------
+    stages = stage_times(pme, s, x_dev, f_dev, stride, recip, stream, flush)
+    G = s.nfft[0] * s.nfft[1] * s.nfft[2]
+    H = (s.nfft[0] // 2 + 1) * s.nfft[1] * s.nfft[2]
+    alg = {"spread": 16 * n + 4 * G, "r2c_fft": 4 * G + 8 * H, "scalar_sum": 16 * H,
+           "c2r_fft": 8 * H + 4 * G, "gather": 28 * n + 4 * G, "self_energy": 16 * n}
+    dom = max(stages, key=lambda k: stages[k])
+    peak, peak_kind = measured_peak()
+    achieved = alg[dom] / (stages[dom] * 1e-3) / 1e9
+    eval_ms = total_ms / K
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
+                "alg_bytes_per_launch": alg[dom], "stage_us": {k: v * 1000 for k, v in stages.items()}}
+    roofline_eval = {"achieved": s.alg_bytes() / (eval_ms * 1e-3) / 1e9, "peak": peak,
+                     "frac": s.alg_bytes() / (eval_ms * 1e-3) / 1e9 / peak, "unit": "GB/s"}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        rate, cnt, dt, cores = cpu_oracle_rate(s, args.cpu_seconds)
+        cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": f"{cnt} full FP64 evaluations of the workload ({dt:.1f} s)"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
+                "warmup": args.warmup, "ms_per_step": total_ms / K, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32+i64 fixed-point grid",
+                "data": "synthetic (seeded TIP3P-geometry water)",
+                "config": workload_config(s, {"parallelism": f"replicas x{world}" if world > 1 else "single GPU"}),
+                "latency_ms": {"p50": float(np.percentile(per, 50)), "p99": float(np.percentile(per, 99))},
+                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 16 * n,
+                        "d2h_bytes_per_step": 4 * 3 * stride + 8 * 11},
+                "gpu_launches": kernels_per_eval * K,
+                "roofline": roofline, "roofline_eval": roofline_eval,
+                "clocks": clocks.summary(), "cpu_baseline": cpu}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def stage_times(pme, s, x, f, stride, recip, stream, flush, reps: int = 50):
+    import torch
+    names = ["spread", "r2c_fft", "scalar_sum", "c2r_fft", "gather", "self_energy"]
+    acc = {k: 0.0 for k in names}
+    n = s.natom
+    with torch.cuda.stream(stream):
+        for r in range(reps + 3):
+            flush.fill_(0.0)
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(len(names) + 1)]
+            ev[0].record(stream)
+            pme.spread_charge(x, n, recip); ev[1].record(stream)
+            pme.r2c_fft(); ev[2].record(stream)
+            pme.scalar_sum(recip, s.kappa, True, True); ev[3].record(stream)
+            pme.c2r_fft(); ev[4].record(stream)
+            pme.gather_force(x, n, recip, stride, f); ev[5].record(stream)
+            pme.calc_self_energy(x, n, s.kappa); ev[6].record(stream)
+            stream.synchronize()
+            if r >= 3:
+                for i, k in enumerate(names):
+                    acc[k] += ev[i].elapsed_time(ev[i + 1])
+    return {k: v / reps for k, v in acc.items()}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

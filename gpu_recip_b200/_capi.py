@@ -1,0 +1,107 @@
+"""ctypes bindings of the C ABI in include/pme_recip.h (libpme_b200.so).
+
+The shared library is built in-tree by gpu_recip_b200/build.py.  There is no fallback: if the
+library is missing or fails to load, every entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "libpme_b200.so")
+
+PME_OK = 0
+PME_EINVAL = -1
+PME_EUNSUPPORTED = -2
+PME_ECUDA = -3
+PME_ETIMEOUT = -4
+PME_ENOMEM = -5
+PME_ESTATE = -6
+
+PME_FFT_COLUMN, PME_FFT_SLAB, PME_FFT_BOX = 0, 1, 2
+PME_FORCE_F32_SOA, PME_FORCE_F32X3, PME_FORCE_I64_SOA_ACCUM = 0, 1, 2
+PME_EV_RECIP, PME_EV_SELF, PME_EV_VIRIAL, PME_EV_COUNT = 0, 1, 2, 11
+
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_D = ctypes.c_double
+_DP = ctypes.POINTER(ctypes.c_double)
+
+# name -> argtypes; every function returns int unless listed in _RESTYPES
+SIGNATURES = {
+    "pme_create": [_I, _I, _I, _I, _I, _I, _I, _P, ctypes.POINTER(_P)],
+    "pme_destroy": [_P],
+    "pme_set_stream": [_P, _P],
+    "pme_set_order": [_P, _I],
+    "pme_get_nfft": [_P, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I)],
+    "pme_get_order": [_P, ctypes.POINTER(_I)],
+    "pme_print_info": [_P],
+    "pme_spread_charge": [_P, _P, _I, _DP],
+    "pme_r2c_fft": [_P],
+    "pme_scalar_sum": [_P, _DP, _D, _I, _I],
+    "pme_c2r_fft": [_P],
+    "pme_gather_force": [_P, _P, _I, _DP, _I, _I, _P],
+    "pme_calc_self_energy": [_P, _P, _I, _D],
+    "pme_clear_energy_virial": [_P],
+    "pme_get_energy_virial": [_P, _DP, _DP, _DP],
+    "pme_copy_energy_virial_async": [_P, _P],
+    "pme_energy_virial_device_ptr": [_P, ctypes.POINTER(_P)],
+    "pme_eval_ortho": [_P, _D, _D, _D, _P, _I, _D, _I, _I, _I, _P, _I],
+    "pme_copy_charge_grid_fixed": [_P, _P],
+    "pme_copy_charge_grid": [_P, _P],
+    "pme_copy_fft_grid": [_P, _P],
+    "pme_copy_solved_grid": [_P, _P],
+    "pme_load_charge_grid": [_P, _P],
+    "pme_last_error_string": [],
+    "pme_status_string": [_I],
+    "pme_version": [],
+}
+_RESTYPES = {"pme_last_error_string": ctypes.c_char_p, "pme_status_string": ctypes.c_char_p}
+
+_lib = None
+
+
+class PMEError(RuntimeError):
+    def __init__(self, status: int, where: str, msg: str):
+        super().__init__(f"{where}: {status_name(status)} ({status}): {msg}")
+        self.status = status
+
+
+def load(path: str | None = None):
+    """Load libpme_b200.so (raises if it is absent: there is no CPU fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise RuntimeError(f"CUDA library {p} is missing; build it with python -m gpu_recip_b200.build")
+    lib = ctypes.CDLL(p)
+    for name, args in SIGNATURES.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = _RESTYPES.get(name, _I)
+    _lib = lib
+    return lib
+
+
+def status_name(status: int) -> str:
+    try:
+        return load().pme_status_string(status).decode()
+    except Exception:  # library not loadable while formatting an error
+        return str(status)
+
+
+def check(status: int, where: str) -> None:
+    if status != PME_OK:
+        msg = load().pme_last_error_string().decode(errors="replace")
+        raise PMEError(status, where, msg)
+
+
+def dbl9(values) -> ctypes.Array:
+    arr = (ctypes.c_double * 9)(*[float(v) for v in values])
+    return arr
+
+
+def exported_symbols():
+    return list(SIGNATURES)

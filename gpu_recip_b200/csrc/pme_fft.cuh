@@ -1,0 +1,151 @@
+// pme_fft.cuh -- shared-memory mixed-radix FFT engine for the 3-D PME transforms (sm_100a).
+//
+// A CTA owns a tile of TX lines of length L, held in shared memory with element e of line t at
+// buf[e * ld + t] (ld >= TX; consecutive threads work on consecutive lines, so shared-memory
+// accesses are conflict free).  The transform is a Stockham autosort FFT: stage s with radix R
+// reads butterfly j's inputs at j + r*L/R, twiddles them by W_{Ns R}^{r k} (k = j mod Ns), does an
+// R-point DFT in registers and writes the outputs at (j div Ns) Ns R + k + u Ns, ping-ponging
+// between two buffers.  Radices 2, 3, 4, 5 cover every 2/3/5-smooth length.  Twiddles
+// W_L^i = exp(-2 pi i i/L) are read from a per-length table computed in FP64 on the host and
+// rounded to FP32.  sign = -1 forward, +1 inverse; transforms are unnormalised.
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace pme {
+
+constexpr int kMaxStages = 12;
+constexpr int kMaxFftLen = 512;
+
+struct FftPlan1D {
+  int n;                    // transform length
+  int nstages;
+  int radix[kMaxStages];
+  int tw_off;               // offset of this length's table in the twiddle array
+};
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(__fsub_rn(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y)),
+                     __fadd_rn(__fmul_rn(a.x, b.y), __fmul_rn(a.y, b.x)));
+}
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+// s * i * a for s = +1 / -1:  i (x + i y) = -y + i x
+__device__ __forceinline__ float2 cmul_si(float2 a, bool inv) {
+  return inv ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
+}
+
+// R-point DFTs in registers.  Forward uses W_R = exp(-2 pi i / R); inverse its conjugate.
+template <int R> __device__ __forceinline__ void dft_small(float2* v, bool inv);
+
+template <> __device__ __forceinline__ void dft_small<2>(float2* v, bool) {
+  float2 a = cadd(v[0], v[1]), b = csub(v[0], v[1]);
+  v[0] = a; v[1] = b;
+}
+
+template <> __device__ __forceinline__ void dft_small<4>(float2* v, bool inv) {
+  float2 a0 = cadd(v[0], v[2]), a1 = csub(v[0], v[2]);
+  float2 b0 = cadd(v[1], v[3]), b1 = csub(v[1], v[3]);
+  float2 jb1 = cmul_si(b1, inv);          // forward: -i b1, inverse: +i b1
+  v[0] = cadd(a0, b0);
+  v[2] = csub(a0, b0);
+  v[1] = cadd(a1, jb1);
+  v[3] = csub(a1, jb1);
+}
+
+template <> __device__ __forceinline__ void dft_small<3>(float2* v, bool inv) {
+  const float h = 0.866025403784438646763723f;   // sin(2 pi/3)
+  float2 s = cadd(v[1], v[2]), d = csub(v[1], v[2]);
+  float2 m = make_float2(v[0].x - 0.5f * s.x, v[0].y - 0.5f * s.y);
+  float2 jd = cmul_si(d, inv);                    // forward: -i d
+  v[0] = cadd(v[0], s);
+  v[1] = make_float2(m.x + h * jd.x, m.y + h * jd.y);
+  v[2] = make_float2(m.x - h * jd.x, m.y - h * jd.y);
+}
+
+template <> __device__ __forceinline__ void dft_small<5>(float2* v, bool inv) {
+  const float c1 = 0.309016994374947424102293f;   // cos(2 pi/5)
+  const float c2 = -0.809016994374947424102293f;  // cos(4 pi/5)
+  const float s1 = 0.951056516295153572116439f;   // sin(2 pi/5)
+  const float s2 = 0.587785252292473129168706f;   // sin(4 pi/5)
+  float2 a1 = cadd(v[1], v[4]), b1 = csub(v[1], v[4]);
+  float2 a2 = cadd(v[2], v[3]), b2 = csub(v[2], v[3]);
+  float2 x0 = v[0];
+  float2 r1 = make_float2(x0.x + c1 * a1.x + c2 * a2.x, x0.y + c1 * a1.y + c2 * a2.y);
+  float2 r2 = make_float2(x0.x + c2 * a1.x + c1 * a2.x, x0.y + c2 * a1.y + c1 * a2.y);
+  float2 t1 = make_float2(s1 * b1.x + s2 * b2.x, s1 * b1.y + s2 * b2.y);
+  float2 t2 = make_float2(s2 * b1.x - s1 * b2.x, s2 * b1.y - s1 * b2.y);
+  float2 j1 = cmul_si(t1, inv), j2 = cmul_si(t2, inv);   // forward: -i t
+  v[0] = make_float2(x0.x + a1.x + a2.x, x0.y + a1.y + a2.y);
+  v[1] = cadd(r1, j1);
+  v[4] = csub(r1, j1);
+  v[2] = cadd(r2, j2);
+  v[3] = csub(r2, j2);
+}
+
+// Thread placement inside a tile: line t = tid mod tx, butterfly lane y = tid div tx (lanes
+// 0..ny-1; threads beyond tx*ny idle during stages).
+struct TileLane {
+  int t, y, ny;
+  __device__ __forceinline__ TileLane(int tid, int nthreads, int tx) {
+    t = tid % tx;
+    y = tid / tx;
+    ny = nthreads / tx;
+  }
+  __device__ __forceinline__ bool active() const { return y < ny; }
+};
+
+// One Stockham stage over all lines of the tile.
+template <int R>
+__device__ __forceinline__ void fft_stage(const float2* __restrict__ in, float2* __restrict__ out,
+                                          int L, int Ns, int ld, const TileLane& ln,
+                                          const float2* tw, bool inv) {
+  const int nb = L / R;
+  const int tstride = L / (Ns * R);
+  const int t = ln.t;
+  if (!ln.active()) return;
+  for (int j = ln.y; j < nb; j += ln.ny) {
+    const int k = j % Ns;
+    float2 v[R];
+#pragma unroll
+    for (int r = 0; r < R; r++) v[r] = in[(j + r * nb) * ld + t];
+#pragma unroll
+    for (int r = 1; r < R; r++) {
+      float2 w = tw[r * k * tstride];
+      if (inv) w.y = -w.y;
+      v[r] = cmul(v[r], w);
+    }
+    dft_small<R>(v, inv);
+    const int base = (j / Ns) * Ns * R + k;
+#pragma unroll
+    for (int u = 0; u < R; u++) out[(base + u * Ns) * ld + t] = v[u];
+  }
+}
+
+// Full transform of the tile held in buf0; returns the buffer that holds the result (buf0 or
+// buf1).  Every thread of the CTA must call it; it synchronises between stages and before
+// returning.
+__device__ __forceinline__ float2* fft_tile(float2* buf0, float2* buf1, const FftPlan1D& plan,
+                                            int ld, const TileLane& ln, const float2* tw,
+                                            bool inv) {
+  float2* src = buf0;
+  float2* dst = buf1;
+  int Ns = 1;
+  const int L = plan.n;
+  for (int s = 0; s < plan.nstages; s++) {
+    const int R = plan.radix[s];
+    switch (R) {
+      case 4: fft_stage<4>(src, dst, L, Ns, ld, ln, tw, inv); break;
+      case 2: fft_stage<2>(src, dst, L, Ns, ld, ln, tw, inv); break;
+      case 3: fft_stage<3>(src, dst, L, Ns, ld, ln, tw, inv); break;
+      case 5: fft_stage<5>(src, dst, L, Ns, ld, ln, tw, inv); break;
+      default: break;
+    }
+    __syncthreads();
+    float2* tmp = src; src = dst; dst = tmp;
+    Ns *= R;
+  }
+  return src;
+}
+
+}  // namespace pme

@@ -1,0 +1,272 @@
+"""Python mirror of the reference operator interface for the PME reciprocal path.
+
+``CudaPMERecip`` follows CudaPMERecip<AT,CT,CT2> (ap-hynninen/gpu_recip, CudaPMERecip.h:166-203)
+method for method -- spread_charge, r2c_fft, scalar_sum, c2r_fft, gather_force,
+calc_self_energy, set_stream, set_order, get_nfft{x,y,z}, get_order, print_info -- and
+``CudaDomdecRecip`` follows the MD adapter (CudaDomdecRecip.h:9-83).  Energy and virial live in
+an ``EnergyVirial`` record that accumulates like CudaEnergyVirial (insert/clear/copyToHost/
+getEnergy/getVirial, CudaEnergyVirial.h:13-53).
+
+All compute runs in libpme_b200.so (hand-written sm_100a kernels) through the C ABI of
+include/pme_recip.h; torch is used only to hold device memory and streams.  Device arrays are
+torch CUDA tensors: xyzq float32 (N, 4) [x, y, z, q]; forces float32 SoA (3*stride,) or
+(3, stride), float32 AoS (N, 3), or int64 SoA fixed point (accumulated, scale 2^40).
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _capi as C
+
+FFT_COLUMN, FFT_SLAB, FFT_BOX = C.PME_FFT_COLUMN, C.PME_FFT_SLAB, C.PME_FFT_BOX
+CCELEC = 332.0716
+FORCE_SCALE = float(1 << 40)
+
+
+def recip_from_box(box: Sequence[float]) -> list:
+    """Row-major 3x3 reciprocal box of an orthorhombic box (CudaDomdecRecip.h:17-23)."""
+    bx, by, bz = (float(b) for b in box)
+    return [1.0 / bx, 0.0, 0.0, 0.0, 1.0 / by, 0.0, 0.0, 0.0, 1.0 / bz]
+
+
+def force_stride(n: int, itemsize: int = 4) -> int:
+    """SoA force stride padded to 256 bytes, as Force<T> (Force.h:63-69)."""
+    return ((((n - 1 + 32) * itemsize) - 1) // 256 + 1) * 256 // itemsize
+
+
+def _stream_handle(stream) -> int:
+    if stream is None:
+        return 0
+    if isinstance(stream, int):
+        return stream
+    return int(stream.cuda_stream)  # torch.cuda.Stream
+
+
+def _ptr(t) -> ctypes.c_void_p:
+    if t is None:
+        return ctypes.c_void_p(0)
+    if isinstance(t, int):
+        return ctypes.c_void_p(t)
+    if not t.is_cuda:
+        raise ValueError("device tensor expected")
+    if not t.is_contiguous():
+        raise ValueError("contiguous tensor expected")
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _xyzq_ptr(xyzq, ncoord: int):
+    import torch
+    if isinstance(xyzq, int):
+        return ctypes.c_void_p(xyzq)
+    if xyzq.dtype != torch.float32:
+        raise ValueError("xyzq must be float32 (x, y, z, q)")
+    if xyzq.numel() < 4 * ncoord:
+        raise ValueError("xyzq holds fewer than ncoord atoms")
+    return _ptr(xyzq)
+
+
+class EnergyVirial:
+    """Energy/virial record (accumulating), the CudaEnergyVirial role for the PME terms."""
+
+    def __init__(self):
+        self._owner: Optional["CudaPMERecip"] = None
+        self._names = {}
+        self._host = np.zeros(C.PME_EV_COUNT)
+
+    def insert(self, name: str, slot: int):
+        self._names[name] = slot
+
+    def _bind(self, owner: "CudaPMERecip"):
+        self._owner = owner
+
+    def clear(self):
+        if self._owner is not None:
+            C.check(C.load().pme_clear_energy_virial(self._owner._h), "clear")
+        self._host[:] = 0.0
+
+    def copyToHost(self):
+        e = ctypes.c_double()
+        s = ctypes.c_double()
+        v = (ctypes.c_double * 9)()
+        C.check(C.load().pme_get_energy_virial(self._owner._h, ctypes.byref(e), ctypes.byref(s), v),
+                "copyToHost")
+        self._host[C.PME_EV_RECIP] = e.value
+        self._host[C.PME_EV_SELF] = s.value
+        self._host[C.PME_EV_VIRIAL:] = np.array(v[:])
+
+    def getEnergy(self, name: str) -> float:
+        return float(self._host[self._names[name]])
+
+    def getVirial(self) -> np.ndarray:
+        return self._host[C.PME_EV_VIRIAL:].reshape(3, 3).copy()
+
+    def copy_async(self, dst) -> None:
+        """Enqueue a copy of the record (11 doubles) into ``dst`` (pinned host or device tensor)."""
+        C.check(C.load().pme_copy_energy_virial_async(self._owner._h, ctypes.c_void_p(dst.data_ptr())),
+                "copy_async")
+
+    def device_ptr(self) -> int:
+        p = ctypes.c_void_p()
+        C.check(C.load().pme_energy_virial_device_ptr(self._owner._h, ctypes.byref(p)), "ev ptr")
+        return int(p.value)
+
+
+class CudaPMERecip:
+    """B200 smooth-PME reciprocal operator (int64 fixed-point grid, FP32 FFT/solve/gather)."""
+
+    def __init__(self, nfftx: int, nffty: int, nfftz: int, order: int, fft_type: int = FFT_BOX,
+                 nnode: int = 1, mynode: int = 0, energy_virial: Optional[EnergyVirial] = None,
+                 name_recip: str = "recip", name_self: str = "self", stream=None):
+        lib = C.load()
+        h = ctypes.c_void_p()
+        C.check(lib.pme_create(nfftx, nffty, nfftz, order, fft_type, nnode, mynode,
+                               ctypes.c_void_p(_stream_handle(stream)), ctypes.byref(h)),
+                "CudaPMERecip")
+        self._h = h
+        self._lib = lib
+        self.nfft = (nfftx, nffty, nfftz)
+        self.energy_virial = energy_virial if energy_virial is not None else EnergyVirial()
+        self.energy_virial.insert(name_recip, C.PME_EV_RECIP)
+        self.energy_virial.insert(name_self, C.PME_EV_SELF)
+        self.energy_virial._bind(self)
+
+    # -- lifetime -------------------------------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self._lib.pme_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- configuration --------------------------------------------------------------------------
+    def set_stream(self, stream):
+        C.check(self._lib.pme_set_stream(self._h, ctypes.c_void_p(_stream_handle(stream))), "set_stream")
+
+    def set_order(self, order: int):
+        C.check(self._lib.pme_set_order(self._h, order), "set_order")
+
+    def get_nfftx(self):
+        return self.nfft[0]
+
+    def get_nffty(self):
+        return self.nfft[1]
+
+    def get_nfftz(self):
+        return self.nfft[2]
+
+    def get_order(self) -> int:
+        o = ctypes.c_int()
+        C.check(self._lib.pme_get_order(self._h, ctypes.byref(o)), "get_order")
+        return o.value
+
+    def print_info(self):
+        C.check(self._lib.pme_print_info(self._h), "print_info")
+
+    # -- stages ---------------------------------------------------------------------------------
+    def spread_charge(self, xyzq, ncoord: int, recip):
+        C.check(self._lib.pme_spread_charge(self._h, _xyzq_ptr(xyzq, ncoord), ncoord, C.dbl9(recip)),
+                "spread_charge")
+
+    def r2c_fft(self):
+        C.check(self._lib.pme_r2c_fft(self._h), "r2c_fft")
+
+    def scalar_sum(self, recip, kappa: float, calc_energy: bool, calc_virial: bool):
+        C.check(self._lib.pme_scalar_sum(self._h, C.dbl9(recip), float(kappa), int(calc_energy),
+                                         int(calc_virial)), "scalar_sum")
+
+    def c2r_fft(self):
+        C.check(self._lib.pme_c2r_fft(self._h), "c2r_fft")
+
+    @staticmethod
+    def _force_kind(force, stride: int):
+        import torch
+        if force.dtype == torch.int64:
+            return C.PME_FORCE_I64_SOA_ACCUM
+        if force.dtype != torch.float32:
+            raise ValueError("force must be float32 or int64")
+        if force.dim() == 2 and force.shape[1] == 3 and stride in (1, 0):
+            return C.PME_FORCE_F32X3
+        return C.PME_FORCE_F32_SOA
+
+    def gather_force(self, xyzq, ncoord: int, recip, stride: int, force, kind: Optional[int] = None):
+        k = self._force_kind(force, stride) if kind is None else kind
+        if k != C.PME_FORCE_F32X3 and force.numel() < 2 * stride + ncoord:
+            raise ValueError("force too small for 3 strided blocks")
+        C.check(self._lib.pme_gather_force(self._h, _xyzq_ptr(xyzq, ncoord), ncoord, C.dbl9(recip),
+                                           int(stride), k, _ptr(force)), "gather_force")
+
+    def calc_self_energy(self, xyzq, ncoord: int, kappa: float):
+        C.check(self._lib.pme_calc_self_energy(self._h, _xyzq_ptr(xyzq, ncoord), ncoord, float(kappa)),
+                "calc_self_energy")
+
+    # -- fused evaluation (CudaDomdecRecip::calc) -----------------------------------------------
+    def eval_ortho(self, inv_box, xyzq, ncoord: int, kappa: float, calc_energy: bool,
+                   calc_virial: bool, force, stride: int = 0, kind: Optional[int] = None):
+        k = self._force_kind(force, stride) if kind is None else kind
+        C.check(self._lib.pme_eval_ortho(self._h, float(inv_box[0]), float(inv_box[1]),
+                                         float(inv_box[2]), _xyzq_ptr(xyzq, ncoord), ncoord,
+                                         float(kappa), int(calc_energy), int(calc_virial), k,
+                                         _ptr(force), int(stride)), "eval_ortho")
+
+    # -- grid read-back (synchronising) ---------------------------------------------------------
+    def charge_grid_fixed(self) -> np.ndarray:
+        nx, ny, nz = self.nfft
+        out = np.empty((nz, ny, nx), dtype=np.int64)
+        C.check(self._lib.pme_copy_charge_grid_fixed(self._h, out.ctypes.data_as(ctypes.c_void_p)),
+                "charge_grid_fixed")
+        return out
+
+    def charge_grid(self) -> np.ndarray:
+        nx, ny, nz = self.nfft
+        out = np.empty((nz, ny, nx), dtype=np.float32)
+        C.check(self._lib.pme_copy_charge_grid(self._h, out.ctypes.data_as(ctypes.c_void_p)),
+                "charge_grid")
+        return out
+
+    def fft_grid(self) -> np.ndarray:
+        nx, ny, nz = self.nfft
+        out = np.empty((nz, ny, nx // 2 + 1, 2), dtype=np.float32)
+        C.check(self._lib.pme_copy_fft_grid(self._h, out.ctypes.data_as(ctypes.c_void_p)), "fft_grid")
+        return out.view(np.complex64)[..., 0]
+
+    def load_charge_grid(self, grid: np.ndarray):
+        nx, ny, nz = self.nfft
+        g = np.ascontiguousarray(grid, dtype=np.float32).reshape(nz, ny, nx)
+        C.check(self._lib.pme_load_charge_grid(self._h, g.ctypes.data_as(ctypes.c_void_p)),
+                "load_charge_grid")
+
+    def solved_grid(self) -> np.ndarray:
+        nx, ny, nz = self.nfft
+        out = np.empty((nz, ny, nx), dtype=np.float32)
+        C.check(self._lib.pme_copy_solved_grid(self._h, out.ctypes.data_as(ctypes.c_void_p)),
+                "solved_grid")
+        return out
+
+
+class CudaDomdecRecip:
+    """MD adapter: calc(inv_box..., coord, ncoord, calc_energy, calc_virial, force) runs the whole
+    reciprocal evaluation (CudaDomdecRecip.h:50-81).  ``force`` may be an int64 SoA fixed-point
+    array (accumulated), a float32 SoA array (overwritten) or a float32 (N, 3) array."""
+
+    def __init__(self, nfftx, nffty, nfftz, order, kappa, energy_virial=None, name_recip="recip",
+                 name_self="self", stream=None):
+        self.kappa = float(kappa)
+        self.pme = CudaPMERecip(nfftx, nffty, nfftz, order, FFT_BOX, 1, 0, energy_virial,
+                                name_recip, name_self, stream)
+
+    def set_stream(self, stream):
+        self.pme.set_stream(stream)
+
+    def calc(self, inv_boxx, inv_boxy, inv_boxz, coord, ncoord, calc_energy, calc_virial, force,
+             stride: Optional[int] = None):
+        if stride is None:
+            stride = 1 if (force.dim() == 2 and force.shape[1] == 3) else force.numel() // 3
+        self.pme.eval_ortho((inv_boxx, inv_boxy, inv_boxz), coord, ncoord, self.kappa, calc_energy,
+                            calc_virial, force, stride)

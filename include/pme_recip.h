@@ -1,0 +1,121 @@
+/* pme_recip.h -- C ABI of the B200 smooth-PME reciprocal-space engine.
+ *
+ * Drop-in for the operator surface of the reference class CudaPMERecip<AT,CT,CT2>
+ * (ap-hynninen/gpu_recip, CudaPMERecip.h:37-205) and of its MD adapter CudaDomdecRecip
+ * (CudaDomdecRecip.h:9-83).  Plain pointers and sizes only; every device pointer argument is a
+ * CUDA device address, every call is asynchronous on the handle's stream unless it says it
+ * synchronises.  Units: Angstrom, elementary charge, kcal/mol (ccelec = 332.0716).
+ *
+ * Differences from the reference, by design:
+ *  - errors are returned as a status code (never exit()); pme_last_error_string() explains;
+ *  - the charge grid is always accumulated in int64 fixed point (scale 2^40), so it is exact
+ *    and run-to-run deterministic; energy and virial reductions are deterministic too;
+ *  - the energy/virial record is owned by the handle (slots "recip" and "self" plus a 3x3
+ *    virial), accumulated like CudaEnergyVirial and cleared with pme_clear_energy_virial().
+ */
+#ifndef PME_RECIP_H
+#define PME_RECIP_H
+
+#if defined(__GNUC__)
+#define PME_API __attribute__((visibility("default")))
+#else
+#define PME_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct pme_recip pme_recip;      /* opaque operator instance */
+
+typedef enum {
+  PME_OK = 0,
+  PME_EINVAL = -1,        /* bad argument (null pointer, size, order, non-orthorhombic box) */
+  PME_EUNSUPPORTED = -2,  /* valid but not supported (grid length with a prime factor > 5) */
+  PME_ECUDA = -3,         /* CUDA runtime error */
+  PME_ETIMEOUT = -4,      /* a bounded wait gave up */
+  PME_ENOMEM = -5,        /* device or host allocation failed */
+  PME_ESTATE = -6         /* call out of order (e.g. no handle state for the request) */
+} pme_status;
+
+/* FFT decomposition of the reference (CudaPMERecip.h:30).  On one GPU all three give the same
+ * result; this engine always runs its own single-GPU 3-D transform. */
+typedef enum { PME_FFT_COLUMN = 0, PME_FFT_SLAB = 1, PME_FFT_BOX = 2 } pme_fft_type;
+
+/* Force output kinds of gather_force<FT> (CudaPMERecip.cu:983-1024). */
+typedef enum {
+  PME_FORCE_F32_SOA = 0,       /* float x|y|z blocks at force, force+stride, force+2*stride; overwrite */
+  PME_FORCE_F32X3 = 1,         /* float3 array (AoS); overwrite; stride ignored */
+  PME_FORCE_I64_SOA_ACCUM = 2  /* long long fixed point 2^40, SoA with stride; atomically ADDED */
+} pme_force_kind;
+
+/* Energy/virial record slots (doubles), device resident. */
+enum { PME_EV_RECIP = 0, PME_EV_SELF = 1, PME_EV_VIRIAL = 2, PME_EV_COUNT = 11 };
+
+/* ---- lifetime (CudaPMERecip ctor/dtor, CudaPMERecip.h:166-170, CudaPMERecip.cu:1411-1493) ---- */
+/* nnode must be 1 and mynode 0 (single GPU).  order in {4, 6, 8}; every grid length must be
+ * 2/3/5-smooth, >= order and <= 512.  stream: cudaStream_t (0 = legacy default stream). */
+PME_API int pme_create(int nfftx, int nffty, int nfftz, int order, int fft_type, int nnode, int mynode,
+               void* stream, pme_recip** out);
+PME_API int pme_destroy(pme_recip* h);
+
+/* ---- configuration (CudaPMERecip.h:176-178, :198-201) ---- */
+PME_API int pme_set_stream(pme_recip* h, void* stream);
+PME_API int pme_set_order(pme_recip* h, int order);                 /* recomputes the B-spline moduli */
+PME_API int pme_get_nfft(const pme_recip* h, int* nfftx, int* nffty, int* nfftz);
+PME_API int pme_get_order(const pme_recip* h, int* order);
+PME_API int pme_print_info(const pme_recip* h);                    /* to stdout (CudaPMERecip.cu:1710) */
+
+/* ---- stages (CudaPMERecip.h:180-197) ----
+ * xyzq: device float4[ncoord] (x, y, z, q).  recip: HOST double[9], row-major 3x3 reciprocal
+ * box; only orthorhombic boxes are accepted (off-diagonals must be 0, as the reference). */
+PME_API int pme_spread_charge(pme_recip* h, const void* xyzq, int ncoord, const double* recip);
+PME_API int pme_r2c_fft(pme_recip* h);
+PME_API int pme_scalar_sum(pme_recip* h, const double* recip, double kappa, int calc_energy,
+                   int calc_virial);
+PME_API int pme_c2r_fft(pme_recip* h);
+/* gather_force<FT>: force is a device pointer of the kind's element type. */
+PME_API int pme_gather_force(pme_recip* h, const void* xyzq, int ncoord, const double* recip, int stride,
+                     int kind, void* force);
+PME_API int pme_calc_self_energy(pme_recip* h, const void* xyzq, int ncoord, double kappa);
+
+/* ---- energy / virial record (CudaEnergyVirial.h:13-53) ---- */
+PME_API int pme_clear_energy_virial(pme_recip* h);                 /* async memset on the stream */
+/* Synchronises the stream, then copies.  Any output pointer may be NULL. */
+PME_API int pme_get_energy_virial(pme_recip* h, double* energy_recip, double* energy_self,
+                          double* virial9);
+/* Enqueue a copy of the record (double[PME_EV_COUNT]) to dst (host pinned or device memory)
+ * on the stream, without synchronising. */
+PME_API int pme_copy_energy_virial_async(pme_recip* h, double* dst);
+/* Device address of the record: double[PME_EV_COUNT]. */
+PME_API int pme_energy_virial_device_ptr(pme_recip* h, double** dev_ptr);
+
+/* ---- fused evaluation: the CudaDomdecRecip::calc sequence (CudaDomdecRecip.h:17-81) ----
+ * spread, R2C, scalar sum (energy/virial if asked), C2R, gather into `force` of `kind`, and the
+ * self energy when calc_energy.  Energy/virial ACCUMULATE into the record.  Same results as the
+ * staged calls, bit for bit. */
+PME_API int pme_eval_ortho(pme_recip* h, double inv_boxx, double inv_boxy, double inv_boxz,
+                   const void* xyzq, int ncoord, double kappa, int calc_energy, int calc_virial,
+                   int kind, void* force, int stride);
+
+/* ---- grid read-back for parity checks (synchronise the stream; host outputs) ----
+ * Layouts follow the reference: real grids [z][y][x]; half-complex grid [z][y][kx],
+ * kx = 0..nfftx/2, interleaved (re, im). */
+PME_API int pme_copy_charge_grid_fixed(pme_recip* h, long long* host_out);   /* nx*ny*nz int64, 2^40 */
+PME_API int pme_copy_charge_grid(pme_recip* h, float* host_out);             /* nx*ny*nz float */
+PME_API int pme_copy_fft_grid(pme_recip* h, float* host_out);                /* 2*(nx/2+1)*ny*nz float */
+PME_API int pme_copy_solved_grid(pme_recip* h, float* host_out);             /* nx*ny*nz float */
+/* Replace the accumulated charge grid (e.g. to test the transforms on a known grid): host
+ * float nx*ny*nz values rounded to the 2^40 fixed point; synchronous. */
+PME_API int pme_load_charge_grid(pme_recip* h, const float* host_in);
+
+/* ---- errors / version ---- */
+PME_API const char* pme_last_error_string(void);     /* thread-local message of the last failure */
+PME_API const char* pme_status_string(int status);
+PME_API int pme_version(void);                       /* 10000*major + 100*minor + patch */
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PME_RECIP_H */

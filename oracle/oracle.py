@@ -1,0 +1,197 @@
+"""ctypes front end of the CPU oracle (TEST INFRASTRUCTURE ONLY).
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU legs of ``bench.py`` may import this
+module: it is the checker of the CUDA path, never part of it.  The C++ restatement it loads
+(``pme_oracle.cpp``, built by the ``Makefile`` beside it) follows the reference operator
+CudaPMERecip (ap-hynninen/gpu_recip, CudaPMERecip.cu); each C function cites the reference
+lines it restates.
+
+Array conventions (numpy):
+  xyzq      (N, 4)  x, y, z [A], q [e]
+  recip3    (3,)    diagonal of the reciprocal box (1/Lx, 1/Ly, 1/Lz)
+  real grid (nz, ny, nx)            x fastest, as the reference's unpadded grid
+  half grid (nz, ny, nx//2+1) complex128
+  forces    (N, 3)  +dE/dx (the reference's gradient convention)
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liboracle.so")
+_lib = None
+
+CCELEC = 332.0716
+
+
+def build(force: bool = False) -> str:
+    """Compile the oracle with its Makefile (g++; no GPU needed)."""
+    src = os.path.join(_HERE, "pme_oracle.cpp")
+    if force or not os.path.exists(_LIB_PATH) or os.path.getmtime(_LIB_PATH) < os.path.getmtime(src):
+        subprocess.run(["make", "-s", "-C", _HERE, "liboracle.so"], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = ctypes.CDLL(_LIB_PATH)
+        P = ctypes.c_void_p
+        I = ctypes.c_int
+        D = ctypes.c_double
+        L.orc_bspline.argtypes = [I, D, P, P]
+        L.orc_spread_f64.argtypes = [P, I, P, I, I, I, I, P, I]
+        L.orc_spread_fixed.argtypes = [P, I, P, I, I, I, I, P, I]
+        L.orc_fixed_to_float.argtypes = [P, ctypes.c_size_t, P]
+        L.orc_fft1d.argtypes = [P, I, I]
+        L.orc_dft1d.argtypes = [P, P, I, I]
+        L.orc_fft3d_r2c.argtypes = [P, I, I, I, P, I]
+        L.orc_fft3d_c2r.argtypes = [P, I, I, I, P, I]
+        L.orc_bspline_moduli.argtypes = [I, I, P]
+        L.orc_scalar_sum.argtypes = [P, I, I, I, I, P, D, I, P, P, I]
+        L.orc_gather.argtypes = [P, I, P, P, I, I, I, I, P, I]
+        L.orc_self_energy.argtypes = [P, I, D]
+        L.orc_self_energy.restype = D
+        L.orc_eval.argtypes = [P, I, P, I, I, I, I, D, P, P, P, P, I]
+        L.orc_hardware_threads.argtypes = []
+        for name in ("orc_bspline", "orc_spread_f64", "orc_spread_fixed", "orc_fixed_to_float",
+                     "orc_fft1d", "orc_dft1d", "orc_fft3d_r2c", "orc_fft3d_c2r",
+                     "orc_bspline_moduli", "orc_scalar_sum", "orc_gather", "orc_eval",
+                     "orc_hardware_threads"):
+            if name not in ("orc_fixed_to_float",):
+                getattr(L, name).restype = I
+        _lib = L
+    return _lib
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _check(rc: int, what: str):
+    if rc != 0:
+        raise ValueError(f"oracle {what} rejected its arguments (rc={rc})")
+
+
+def hardware_threads() -> int:
+    return int(lib().orc_hardware_threads())
+
+
+def bspline(order: int, u: float):
+    th = np.zeros(order)
+    dth = np.zeros(order)
+    _check(lib().orc_bspline(order, float(u), _p(th), _p(dth)), "bspline")
+    return th, dth
+
+
+def bspline_moduli(order: int, n: int) -> np.ndarray:
+    out = np.zeros(n)
+    _check(lib().orc_bspline_moduli(order, n, _p(out)), "moduli")
+    return out
+
+
+def spread_f64(xyzq, recip3, nfft, order, nthreads=0) -> np.ndarray:
+    x = np.ascontiguousarray(xyzq, dtype=np.float64).reshape(-1, 4)
+    r = np.ascontiguousarray(recip3, dtype=np.float64)
+    nx, ny, nz = nfft
+    g = np.zeros((nz, ny, nx))
+    _check(lib().orc_spread_f64(_p(x), x.shape[0], _p(r), nx, ny, nz, order, _p(g), nthreads),
+           "spread_f64")
+    return g
+
+
+def spread_fixed(xyzq, recip3, nfft, order, nthreads=0) -> np.ndarray:
+    """int64 fixed-point grid (scale 2^40) from the FP32 mirror of the GPU spreading."""
+    x = np.ascontiguousarray(xyzq, dtype=np.float32).reshape(-1, 4)
+    r = np.ascontiguousarray(np.asarray(recip3, dtype=np.float64).astype(np.float32))
+    nx, ny, nz = nfft
+    g = np.zeros((nz, ny, nx), dtype=np.int64)
+    _check(lib().orc_spread_fixed(_p(x), x.shape[0], _p(r), nx, ny, nz, order, _p(g), nthreads),
+           "spread_fixed")
+    return g
+
+
+def fixed_to_float(g: np.ndarray) -> np.ndarray:
+    g = np.ascontiguousarray(g, dtype=np.int64)
+    out = np.empty(g.shape, dtype=np.float32)
+    lib().orc_fixed_to_float(_p(g), g.size, _p(out))
+    return out
+
+
+def fft1d(x, sign=-1) -> np.ndarray:
+    a = np.ascontiguousarray(x, dtype=np.complex128).copy()
+    _check(lib().orc_fft1d(_p(a), a.size, sign), "fft1d")
+    return a
+
+
+def dft1d(x, sign=-1) -> np.ndarray:
+    a = np.ascontiguousarray(x, dtype=np.complex128)
+    out = np.empty_like(a)
+    _check(lib().orc_dft1d(_p(a), _p(out), a.size, sign), "dft1d")
+    return out
+
+
+def fft3d_r2c(grid: np.ndarray, nthreads=0) -> np.ndarray:
+    g = np.ascontiguousarray(grid, dtype=np.float64)
+    nz, ny, nx = g.shape
+    out = np.empty((nz, ny, nx // 2 + 1), dtype=np.complex128)
+    _check(lib().orc_fft3d_r2c(_p(g), nx, ny, nz, _p(out), nthreads), "fft3d_r2c")
+    return out
+
+
+def fft3d_c2r(half: np.ndarray, nx: int, nthreads=0) -> np.ndarray:
+    h = np.ascontiguousarray(half, dtype=np.complex128)
+    nz, ny, hx = h.shape
+    assert hx == nx // 2 + 1
+    out = np.empty((nz, ny, nx))
+    _check(lib().orc_fft3d_c2r(_p(h), nx, ny, nz, _p(out), nthreads), "fft3d_c2r")
+    return out
+
+
+def scalar_sum(half: np.ndarray, nx: int, order: int, recip3, kappa: float, calc_ev=True,
+               nthreads=0):
+    """Returns (solved half grid, energy, virial 3x3)."""
+    h = np.ascontiguousarray(half, dtype=np.complex128).copy()
+    nz, ny, hx = h.shape
+    r = np.ascontiguousarray(recip3, dtype=np.float64)
+    e = np.zeros(1)
+    v = np.zeros(9)
+    _check(lib().orc_scalar_sum(_p(h), nx, ny, nz, order, _p(r), float(kappa), int(calc_ev),
+                                _p(e), _p(v), nthreads), "scalar_sum")
+    return h, float(e[0]), v.reshape(3, 3)
+
+
+def gather(xyzq, grid: np.ndarray, recip3, order, nthreads=0) -> np.ndarray:
+    x = np.ascontiguousarray(xyzq, dtype=np.float64).reshape(-1, 4)
+    g = np.ascontiguousarray(grid, dtype=np.float64)
+    nz, ny, nx = g.shape
+    r = np.ascontiguousarray(recip3, dtype=np.float64)
+    f = np.zeros((x.shape[0], 3))
+    _check(lib().orc_gather(_p(x), x.shape[0], _p(g), _p(r), nx, ny, nz, order, _p(f), nthreads),
+           "gather")
+    return f
+
+
+def self_energy(xyzq, kappa) -> float:
+    x = np.ascontiguousarray(xyzq, dtype=np.float64).reshape(-1, 4)
+    return float(lib().orc_self_energy(_p(x), x.shape[0], float(kappa)))
+
+
+def evaluate(xyzq, recip3, nfft, order, kappa, nthreads=0):
+    """Full FP64 evaluation.  Returns dict(force (N,3), energy, energy_self, virial (3,3))."""
+    x = np.ascontiguousarray(xyzq, dtype=np.float64).reshape(-1, 4)
+    r = np.ascontiguousarray(recip3, dtype=np.float64)
+    nx, ny, nz = nfft
+    f = np.zeros((x.shape[0], 3))
+    e = np.zeros(1)
+    es = np.zeros(1)
+    v = np.zeros(9)
+    _check(lib().orc_eval(_p(x), x.shape[0], _p(r), nx, ny, nz, order, float(kappa), _p(f),
+                          _p(e), _p(es), _p(v), nthreads), "eval")
+    return {"force": f, "energy": float(e[0]), "energy_self": float(es[0]),
+            "virial": v.reshape(3, 3)}
