@@ -24,7 +24,6 @@ import statistics
 import subprocess
 import sys
 import tempfile
-import threading
 import time
 
 import numpy as np
@@ -33,6 +32,10 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "PME recip evals/s at 24k atoms/64^3; batched evals/s + p50/p99 latency, same GPU"
+
+# DRAM bytes (read + write) of one k_fused launch from an ncu capture, by workload (None until
+# captured).  Filled from profiles/ summaries.
+TRAFFIC_BYTES = {}
 UNIT = "evals/s"
 FALLBACK_HBM_GBS = 6650.0
 
@@ -47,6 +50,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="time budget of the cpu_baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batch", type=int, default=256, help="systems in the batched measurement (0: skip)")
+    ap.add_argument("--batch-steps", type=int, default=200)
     return ap.parse_args()
 
 
@@ -228,7 +233,7 @@ def run_b200(args):
         pme.energy_virial.clear()
         pme.eval_ortho(inv_box, x_dev, n, s.kappa, True, True, f_dev, stride)
 
-    kernels_per_eval = 8   # spread, x_r2c, y fwd, z fwd+solve+inv, y inv, x_c2r, gather, self
+    kernels_per_eval = 1   # the fused cooperative kernel (plus one energy/virial memset)
 
     with torch.cuda.stream(stream):
         for _ in range(max(3, args.warmup)):
@@ -289,21 +294,23 @@ def run_b200(args):
         e_total = float(t.item())
     e2e_value = world * Ke / (e_total / 1000.0)
 
-    # ---- per-stage timing (staged C-ABI calls) for the roofline -------------------------------------
+    # ---- staged C-ABI calls, per reference stage (informational) -----------------------------------
     stages = stage_times(pme, s, x_dev, f_dev, stride, recip, stream, flush)
-    G = s.nfft[0] * s.nfft[1] * s.nfft[2]
-    H = (s.nfft[0] // 2 + 1) * s.nfft[1] * s.nfft[2]
-    alg = {"spread": 16 * n + 4 * G, "r2c_fft": 4 * G + 8 * H, "scalar_sum": 16 * H,
-           "c2r_fft": 8 * H + 4 * G, "gather": 28 * n + 4 * G, "self_energy": 16 * n}
-    dom = max(stages, key=lambda k: stages[k])
+
+    # ---- roofline of the dominant kernel: the fused evaluation is one launch -------------------------
     peak, peak_kind = measured_peak()
-    achieved = alg[dom] / (stages[dom] * 1e-3) / 1e9
     eval_ms = total_ms / K
-    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
-                "alg_bytes_per_launch": alg[dom], "stage_us": {k: v * 1000 for k, v in stages.items()}}
-    roofline_eval = {"achieved": s.alg_bytes() / (eval_ms * 1e-3) / 1e9, "peak": peak,
-                     "frac": s.alg_bytes() / (eval_ms * 1e-3) / 1e9 / peak, "unit": "GB/s"}
+    achieved = s.alg_bytes() / (eval_ms * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "kernel": "k_fused (whole evaluation, one cooperative launch)",
+                "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "peak_source": peak_kind, "traffic": TRAFFIC_BYTES.get(args.workload),
+                "alg_bytes_per_launch": s.alg_bytes(),
+                "staged_stage_us": {k: v * 1000 for k, v in stages.items()}}
+
+    # ---- batched: uneven systems in one persistent launch --------------------------------------------
+    batched = None
+    if args.batch > 0:
+        batched = run_batched(args, dev, stream, flush, rank, world)
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -321,12 +328,65 @@ def run_b200(args):
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 16 * n,
                         "d2h_bytes_per_step": 4 * 3 * stride + 8 * 11},
                 "gpu_launches": kernels_per_eval * K,
-                "roofline": roofline, "roofline_eval": roofline_eval,
+                "roofline": roofline, "batched": batched,
                 "clocks": clocks.summary(), "cpu_baseline": cpu}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def run_batched(args, dev, stream, flush, rank, world):
+    """256 independent water boxes of 648-24,000 atoms, 24^3-64^3 grids, order 4, kappa 0.32, all
+    evaluated by one persistent launch per step (L2 flushed before every step)."""
+    import torch
+    import torch.distributed as dist
+    from gpu_recip_b200 import PmeBatch, force_stride
+    from gpu_recip_b200 import systems as S
+    systems = S.batch_systems(args.batch, seed=4 + 1000 * rank)
+    specs = []
+    for sy in systems:
+        x = torch.from_numpy(sy.xyzq).to(dev)
+        st = force_stride(sy.natom)
+        f = torch.zeros(3 * st, dtype=torch.float32, device=dev)
+        specs.append(dict(nfft=sy.nfft, order=sy.order, box=sy.box, kappa=sy.kappa, xyzq=x, force=f, stride=st))
+    b = PmeBatch(specs, stream=stream)
+    with torch.cuda.stream(stream):
+        for _ in range(3):
+            flush.fill_(0.0)
+            b.clear_energy_virial()
+            b.eval()
+    stream.synchronize()
+    K = args.batch_steps
+    st_ev = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    en_ev = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        for i in range(K):
+            flush.fill_(float(i & 7))
+            st_ev[i].record(stream)
+            b.clear_energy_virial()
+            b.eval()
+            en_ev[i].record(stream)
+    stream.synchronize()
+    per = np.array([st_ev[i].elapsed_time(en_ev[i]) for i in range(K)])
+    total = float(per.sum())
+    if world > 1:
+        t = torch.tensor([total], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total = float(t.item())
+    peak, _ = measured_peak()
+    alg = sum(sy.alg_bytes() for sy in systems)
+    ms = total / K
+    info = b.info()
+    return {"systems": len(systems), "atoms": int(sum(sy.natom for sy in systems)),
+            "evals_per_s": world * len(systems) * K / (total / 1000.0), "ms_per_batch": ms,
+            "p50_ms": float(np.percentile(per, 50)), "p99_ms": float(np.percentile(per, 99)),
+            "launches_per_batch": 1, "grid_ctas": info["grid_ctas"],
+            "device_bytes": info["device_bytes"], "alg_bytes_per_batch": alg,
+            "roofline_frac": alg / (ms * 1e-3) / 1e9 / peak}
 
 
 def stage_times(pme, s, x, f, stride, recip, stream, flush, reps: int = 50):

@@ -53,11 +53,37 @@ SIGNATURES = {
     "pme_copy_fft_grid": [_P, _P],
     "pme_copy_solved_grid": [_P, _P],
     "pme_load_charge_grid": [_P, _P],
+    "pme_get_status": [_P, ctypes.POINTER(_I)],
+    "pme_set_barrier_spin_limit": [_P, ctypes.c_uint],
+    "pme_set_fault_injection": [_P, _I],
+    "pme_batch_create": [_P, _I, _P, ctypes.POINTER(_P)],
+    "pme_batch_destroy": [_P],
+    "pme_batch_set_stream": [_P, _P],
+    "pme_batch_set_system": [_P, _I, _DP, _P, _P],
+    "pme_batch_commit": [_P],
+    "pme_batch_eval": [_P],
+    "pme_batch_clear_energy_virial": [_P],
+    "pme_batch_get_energy_virial": [_P, _DP],
+    "pme_batch_info": [_P, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(ctypes.c_size_t)],
+    "pme_system_device_bytes": [_I, _I, _I],
+    "pme_set_trace": [_P, _P, _I],
+    "pme_batch_set_trace": [_P, _P, _I],
     "pme_last_error_string": [],
     "pme_status_string": [_I],
     "pme_version": [],
 }
-_RESTYPES = {"pme_last_error_string": ctypes.c_char_p, "pme_status_string": ctypes.c_char_p}
+_RESTYPES = {"pme_last_error_string": ctypes.c_char_p, "pme_status_string": ctypes.c_char_p,
+             "pme_system_device_bytes": ctypes.c_size_t}
+
+PME_INJECT_NONE, PME_INJECT_SKIP_BARRIER = 0, 1
+
+
+class SystemDesc(ctypes.Structure):
+    """pme_system_desc of include/pme_recip.h."""
+    _fields_ = [("nfftx", _I), ("nffty", _I), ("nfftz", _I), ("order", _I), ("natom", _I),
+                ("box", ctypes.c_double * 3), ("kappa", ctypes.c_double), ("xyzq", _P),
+                ("force", _P), ("force_kind", _I), ("stride", _I), ("calc_energy", _I),
+                ("calc_virial", _I)]
 
 _lib = None
 

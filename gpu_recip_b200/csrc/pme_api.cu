@@ -1,11 +1,12 @@
 // pme_api.cu -- host engine and C ABI of the B200 smooth-PME reciprocal-space operator.
 //
-// One pme_recip instance mirrors one CudaPMERecip<long long, float, float2> of the reference
-// (CudaPMERecip.h:37-205): it owns the int64 accumulation grid, the half-complex FFT grid, the
-// solved real grid, per-axis FFT plans with FP64-accurate twiddles, the FP64-computed B-spline
-// moduli (stored FP32) and the energy/virial record.  Every compute call only enqueues kernels
-// on the instance's stream: no allocation, no host synchronisation, so a whole evaluation can
-// be captured in a CUDA graph.
+// A pme_recip instance mirrors one CudaPMERecip<long long, float, float2> of the reference
+// (CudaPMERecip.h:37-205); a pme_batch holds many independent systems evaluated by one
+// persistent launch.  Both own, per system, the int64 accumulation grid, the half-complex grid,
+// the solved real grid, FFT plans with FP64-accurate twiddles, FP64 B-spline moduli, the FP64
+// influence tables, the fixed-point energy/virial accumulators and the FP64 energy/virial record,
+// carved from one device allocation.  Compute calls only enqueue work on the instance's stream
+// (no allocation, no host synchronisation), so evaluations can be captured in CUDA graphs.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -19,27 +20,7 @@
 #include "../../include/pme_recip.h"
 #include "pme_internal.h"
 
-namespace pme {
-cudaError_t configure_kernels();
-}
-
 using namespace pme;
-
-struct pme_recip {
-  int nx, ny, nz, order, fft_type, device;
-  cudaStream_t stream;
-  FftPlan1D px, py, pz;
-  PassTiling tile_x, tile_y, tile_z;
-  long long* d_accum;
-  float2* d_cgrid;
-  float* d_rgrid;
-  float2* d_tw;
-  float* d_bmod;
-  double* d_ev;
-  double* d_partials;
-  unsigned int* d_ticket;
-  int max_blocks;
-};
 
 namespace {
 
@@ -51,6 +32,7 @@ int fail(int status, const std::string& msg) {
 }
 
 int cuda_fail(cudaError_t e, const char* where) {
+  cudaGetLastError();
   return fail(PME_ECUDA, std::string(where) + ": " + cudaGetErrorString(e));
 }
 
@@ -59,9 +41,7 @@ struct DeviceGuard {
   int prev = -1;
   bool changed = false;
   explicit DeviceGuard(int dev) {
-    if (cudaGetDevice(&prev) == cudaSuccess && prev != dev) {
-      changed = (cudaSetDevice(dev) == cudaSuccess);
-    }
+    if (cudaGetDevice(&prev) == cudaSuccess && prev != dev) changed = (cudaSetDevice(dev) == cudaSuccess);
   }
   ~DeviceGuard() {
     if (changed) cudaSetDevice(prev);
@@ -71,6 +51,7 @@ struct DeviceGuard {
 bool factorize(int n, FftPlan1D& p) {
   p.n = n;
   p.nstages = 0;
+  p.n_div = make_fastdiv(n);
   int m = n;
   auto push = [&](int r) {
     if (p.nstages >= kMaxStages) return false;
@@ -82,10 +63,16 @@ bool factorize(int n, FftPlan1D& p) {
   while (m % 2 == 0) if (!push(2)) return false;
   while (m % 3 == 0) if (!push(3)) return false;
   while (m % 5 == 0) if (!push(5)) return false;
-  return m == 1;
+  if (m != 1) return false;
+  int ns = 1;
+  for (int s = 0; s < p.nstages; s++) {
+    p.ns_div[s] = make_fastdiv(ns);
+    ns *= p.radix[s];
+  }
+  return true;
 }
 
-// Cardinal B-spline weights at u (FP64) by the same recursion as the kernels.
+// Cardinal B-spline weights at u (FP64) by the recursion of CudaPMERecip.cu:2507-2537.
 void bspline_host(int p, double u, double* th) {
   for (int i = 0; i < p; i++) th[i] = 0.0;
   th[0] = 1.0 - u;
@@ -102,7 +89,7 @@ void bspline_host(int p, double u, double* th) {
 // B-spline moduli 1/|b(k)|^2 in FP64 (CudaPMERecip.cu:2481-2505 dftmod, :2543-2579 calc_prefac):
 // DFT over j = 0..n-2 of M = [0, theta_0(0), ..., theta_{p-1}(0), 0, ...]; values below 1e-10
 // take the mean of their neighbours.
-void bspline_moduli(int p, int n, std::vector<float>& out) {
+void bspline_moduli(int p, int n, double* out) {
   std::vector<double> arr((size_t)std::max(n, p + 2), 0.0), th(p), mod(n);
   bspline_host(p, 0.0, th.data());
   for (int i = 1; i <= p; i++) arr[i] = th[i - 1];
@@ -117,140 +104,49 @@ void bspline_moduli(int p, int n, std::vector<float>& out) {
   }
   for (int k = 0; k < n; k++)
     if (mod[k] < 1.0e-10) mod[k] = 0.5 * (mod[(k - 1 + n) % n] + mod[(k + 1) % n]);
-  out.resize(n);
-  for (int k = 0; k < n; k++) out[k] = (float)(1.0 / mod[k]);
+  for (int k = 0; k < n; k++) out[k] = 1.0 / mod[k];
 }
 
-PassTiling pick_tiling_rows(int L) {
-  PassTiling t;
-  t.tx = 16;
-  // keep the tile's two buffers within ~200 KB of shared memory
-  while (t.tx > 1 && sizeof(float2) * ((size_t)L + 2 * (size_t)L * (t.tx + 1)) > 200 * 1024) t.tx--;
-  t.ny = 0;
-  return t;
+constexpr size_t kTileSmemBudget = 100 * 1024;   // keeps >= 2 CTAs per SM for the FFT passes
+
+int pick_rows_tile(int L) {
+  int tx = 16;
+  while (tx > 1 && tile_smem_bytes(L, tx) > kTileSmemBudget) tx--;
+  return tx;
 }
 
-PassTiling pick_tiling_cols(int hx, int L) {
-  PassTiling best;
-  best.tx = 16;
-  best.ny = 0;
-  int best_waste = 1 << 30;
+int pick_cols_tile(int hx, int L) {
+  int best = 16, best_waste = 1 << 30;
   for (int tx = 17; tx >= 8; tx--) {
-    int tiles = (hx + tx - 1) / tx;
-    int waste = tiles * tx - hx;
-    if (waste < best_waste) {
-      best_waste = waste;
-      best.tx = tx;
-    }
+    const int waste = ((hx + tx - 1) / tx) * tx - hx;
+    if (waste < best_waste) { best_waste = waste; best = tx; }
   }
-  if (hx < 8) best.tx = hx;
-  while (best.tx > 1 && sizeof(float2) * ((size_t)L + 2 * (size_t)L * (best.tx + 1)) > 200 * 1024)
-    best.tx--;
+  if (hx < 8) best = hx;
+  while (best > 1 && tile_smem_bytes(L, best) > kTileSmemBudget) best--;
   return best;
-}
-
-bool is_ortho(const double* r) {
-  return r[1] == 0.0 && r[2] == 0.0 && r[3] == 0.0 && r[5] == 0.0 && r[6] == 0.0 && r[7] == 0.0;
-}
-
-int check_recip(const double* recip) {
-  if (!recip) return fail(PME_EINVAL, "recip is NULL");
-  if (!is_ortho(recip))
-    return fail(PME_EINVAL, "only orthorhombic boxes are supported (recip off-diagonals must be 0)");
-  if (!(recip[0] > 0.0 && recip[4] > 0.0 && recip[8] > 0.0) || !std::isfinite(recip[0]) ||
-      !std::isfinite(recip[4]) || !std::isfinite(recip[8]))
-    return fail(PME_EINVAL, "recip diagonal must be finite and positive");
-  return PME_OK;
-}
-
-Geom make_geom(const pme_recip* h, const double* recip) {
-  Geom g;
-  g.nx = h->nx; g.ny = h->ny; g.nz = h->nz;
-  g.hx = h->nx / 2 + 1;
-  g.rx = recip ? (float)recip[0] : 0.0f;
-  g.ry = recip ? (float)recip[4] : 0.0f;
-  g.rz = recip ? (float)recip[8] : 0.0f;
-  return g;
-}
-
-ReduceScratch scratch(const pme_recip* h) {
-  ReduceScratch rs;
-  rs.partials = h->d_partials;
-  rs.ticket = h->d_ticket;
-  rs.max_blocks = h->max_blocks;
-  return rs;
-}
-
-enum { kSiteSolve = 0, kSiteSelf = 1, kNumSites = 4 };
-
-void release(pme_recip* h) {
-  if (!h) return;
-  cudaFree(h->d_accum);
-  cudaFree(h->d_cgrid);
-  cudaFree(h->d_rgrid);
-  cudaFree(h->d_tw);
-  cudaFree(h->d_bmod);
-  cudaFree(h->d_ev);
-  cudaFree(h->d_partials);
-  cudaFree(h->d_ticket);
-  delete h;
-}
-
-int upload_moduli(pme_recip* h) {
-  std::vector<float> bx, by, bz;
-  bspline_moduli(h->order, h->nx, bx);
-  bspline_moduli(h->order, h->ny, by);
-  bspline_moduli(h->order, h->nz, bz);
-  std::vector<float> all;
-  all.insert(all.end(), bx.begin(), bx.end());
-  all.insert(all.end(), by.begin(), by.end());
-  all.insert(all.end(), bz.begin(), bz.end());
-  cudaError_t e = cudaMemcpy(h->d_bmod, all.data(), all.size() * sizeof(float),
-                             cudaMemcpyHostToDevice);
-  if (e != cudaSuccess) return cuda_fail(e, "upload moduli");
-  return PME_OK;
-}
-
-SolveParams solve_params(const pme_recip* h, const double* recip, double kappa, int calc_ev) {
-  SolveParams sp;
-  const double inv_vol = recip[0] * recip[4] * recip[8];
-  sp.fac = (float)(kPi * kPi / (kappa * kappa));
-  sp.piv_inv = (float)(inv_vol / kPi);
-  sp.bmx = h->d_bmod;
-  sp.bmy = h->d_bmod + h->nx;
-  sp.bmz = h->d_bmod + h->nx + h->ny;
-  sp.calc_ev = calc_ev;
-  sp.ev = h->d_ev;
-  return sp;
 }
 
 int valid_order(int order) { return order == 4 || order == 6 || order == 8; }
 
-// Enqueue helpers shared by the staged and fused paths.
-int enqueue_spread(pme_recip* h, const void* xyzq, int ncoord, const Geom& g) {
-  const size_t G = (size_t)h->nx * h->ny * h->nz;
-  cudaError_t e = cudaMemsetAsync(h->d_accum, 0, G * sizeof(long long), h->stream);
-  if (e != cudaSuccess) return cuda_fail(e, "spread_charge: clear grid");
-  e = launch_spread((const float4*)xyzq, ncoord, g, h->order, (unsigned long long*)h->d_accum,
-                    h->stream);
-  if (e != cudaSuccess) return cuda_fail(e, "spread_charge");
+int check_grid(int nx, int ny, int nz, int order) {
+  if (!valid_order(order)) return fail(PME_EINVAL, "order must be 4, 6 or 8");
+  const int n3[3] = {nx, ny, nz};
+  for (int d = 0; d < 3; d++)
+    if (n3[d] < order || n3[d] > kMaxFftLen) return fail(PME_EINVAL, "grid lengths must be in [order, 512]");
+  FftPlan1D p;
+  for (int d = 0; d < 3; d++)
+    if (!factorize(n3[d], p)) return fail(PME_EUNSUPPORTED, "grid lengths must factor into 2, 3 and 5");
   return PME_OK;
 }
 
-int enqueue_r2c(pme_recip* h, const Geom& g) {
-  cudaError_t e = launch_x_r2c(h->d_accum, h->d_cgrid, g, h->px, h->d_tw, h->tile_x, h->stream);
-  if (e != cudaSuccess) return cuda_fail(e, "r2c_fft: x pass");
-  e = launch_c2c(h->d_cgrid, g, 1, 0, h->py, h->d_tw, h->tile_y, nullptr, scratch(h), 0, h->stream);
-  if (e != cudaSuccess) return cuda_fail(e, "r2c_fft: y pass");
-  return PME_OK;
-}
-
-int enqueue_c2r_tail(pme_recip* h, const Geom& g) {
-  cudaError_t e =
-      launch_c2c(h->d_cgrid, g, 1, 1, h->py, h->d_tw, h->tile_y, nullptr, scratch(h), 0, h->stream);
-  if (e != cudaSuccess) return cuda_fail(e, "c2r_fft: y pass");
-  e = launch_x_c2r(h->d_cgrid, h->d_rgrid, g, h->px, h->d_tw, h->tile_x, h->stream);
-  if (e != cudaSuccess) return cuda_fail(e, "c2r_fft: x pass");
+int check_recip(const double* recip) {
+  if (!recip) return fail(PME_EINVAL, "recip is NULL");
+  if (!(recip[1] == 0.0 && recip[2] == 0.0 && recip[3] == 0.0 && recip[5] == 0.0 &&
+        recip[6] == 0.0 && recip[7] == 0.0))
+    return fail(PME_EINVAL, "only orthorhombic boxes are supported (recip off-diagonals must be 0)");
+  for (int i : {0, 4, 8})
+    if (!(recip[i] > 0.0) || !std::isfinite(recip[i]))
+      return fail(PME_EINVAL, "recip diagonal must be finite and positive");
   return PME_OK;
 }
 
@@ -260,6 +156,209 @@ int check_force_args(int ncoord, int stride, int kind, const void* force) {
   if (ncoord > 0 && !force) return fail(PME_EINVAL, "force is NULL");
   if (kind != PME_FORCE_F32X3 && ncoord > 0 && stride < ncoord)
     return fail(PME_EINVAL, "stride must be >= ncoord for strided force layouts");
+  return PME_OK;
+}
+
+size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// Per-system device state, carved from a caller-provided device block.
+struct SystemState {
+  int nx = 0, ny = 0, nz = 0, order = 0;
+  FftPlan1D px{}, py{}, pz{};
+  int tx_rows = 0, tx_y = 0, tx_z = 0;
+  unsigned long long* accum = nullptr;
+  float2* cgrid = nullptr;
+  float* rgrid = nullptr;
+  float2* tw = nullptr;
+  double* bmod = nullptr;
+  double* ktab = nullptr;
+  long long* acc = nullptr;
+  double* ev = nullptr;
+
+  size_t G() const { return (size_t)nx * ny * nz; }
+  size_t H() const { return (size_t)(nx / 2 + 1) * ny * nz; }
+
+  // bytes of device memory one system needs
+  static size_t bytes(int nx, int ny, int nz) {
+    const size_t G = (size_t)nx * ny * nz, H = (size_t)(nx / 2 + 1) * ny * nz, n = nx + ny + nz;
+    return align256(G * 8) + align256(H * 8) + align256(G * 4) + align256(n * 8) + align256(n * 8) +
+           align256(2 * n * 8) + align256(kAccCount * 8) + align256(kEvCount * 8);
+  }
+
+  void setup(int nx_, int ny_, int nz_, int order_) {
+    nx = nx_; ny = ny_; nz = nz_; order = order_;
+    factorize(nx, px);
+    factorize(ny, py);
+    factorize(nz, pz);
+    px.tw_off = 0;
+    py.tw_off = nx;
+    pz.tw_off = nx + ny;
+    tx_rows = pick_rows_tile(nx);
+    tx_y = pick_cols_tile(nx / 2 + 1, ny);
+    tx_z = pick_cols_tile(nx / 2 + 1, nz);
+  }
+
+  void carve(char* base) {
+    const size_t n = nx + ny + nz;
+    char* p = base;
+    accum = (unsigned long long*)p; p += align256(G() * 8);
+    cgrid = (float2*)p; p += align256(H() * 8);
+    rgrid = (float*)p; p += align256(G() * 4);
+    tw = (float2*)p; p += align256(n * 8);
+    bmod = (double*)p; p += align256(n * 8);
+    ktab = (double*)p; p += align256(2 * n * 8);
+    acc = (long long*)p; p += align256(kAccCount * 8);
+    ev = (double*)p;
+  }
+
+  // twiddles exp(-2 pi i k/n) (FP64 -> FP32) and moduli (FP64) for the current order
+  void host_tables(std::vector<float2>& twh, std::vector<double>& bm) const {
+    const int n3[3] = {nx, ny, nz};
+    twh.clear();
+    bm.assign((size_t)(nx + ny + nz), 0.0);
+    size_t off = 0;
+    for (int d = 0; d < 3; d++) {
+      for (int k = 0; k < n3[d]; k++) {
+        const double a = -2.0 * kPi * (double)k / (double)n3[d];
+        twh.push_back(make_float2((float)std::cos(a), (float)std::sin(a)));
+      }
+      bspline_moduli(order, n3[d], bm.data() + off);
+      off += n3[d];
+    }
+  }
+
+  cudaError_t upload_tables() const {
+    std::vector<float2> twh;
+    std::vector<double> bm;
+    host_tables(twh, bm);
+    cudaError_t e = cudaMemcpy(tw, twh.data(), twh.size() * sizeof(float2), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(bmod, bm.data(), bm.size() * sizeof(double), cudaMemcpyHostToDevice);
+    return e;
+  }
+
+  SysDesc desc(const double* r3, double kappa, const void* xyzq, int natom, void* force, int kind,
+               int stride, int calc_ev, int calc_self) const {
+    SysDesc d;
+    std::memset(&d, 0, sizeof(d));
+    Geom& g = d.g;
+    g.nx = nx; g.ny = ny; g.nz = nz;
+    g.hx = nx / 2 + 1;
+    const double r[3] = {r3 ? r3[0] : 1.0, r3 ? r3[1] : 1.0, r3 ? r3[2] : 1.0};
+    g.rx = (float)r[0]; g.ry = (float)r[1]; g.rz = (float)r[2];
+    const int n3[3] = {nx, ny, nz};
+    float hi[3], lo[3];
+    for (int i = 0; i < 3; i++) {
+      const double s = r[i] * n3[i];
+      hi[i] = (float)s;
+      lo[i] = (float)(s - (double)hi[i]);
+    }
+    g.sx_hi = hi[0]; g.sy_hi = hi[1]; g.sz_hi = hi[2];
+    g.sx_lo = lo[0]; g.sy_lo = lo[1]; g.sz_lo = lo[2];
+    d.px = px; d.py = py; d.pz = pz;
+    d.order = order;
+    d.natom = natom;
+    d.rxd = r[0]; d.ryd = r[1]; d.rzd = r[2];
+    d.fac = kappa > 0.0 ? kPi * kPi / (kappa * kappa) : 0.0;
+    d.piv_inv = r[0] * r[1] * r[2] / kPi;
+    d.calc_ev = calc_ev;
+    d.calc_self = calc_self;
+    d.self_coef = -kappa * kCcelec / std::sqrt(kPi);
+    d.force_kind = kind;
+    d.stride = stride;
+    d.xyzq = (const float4*)xyzq;
+    d.force = force;
+    d.accum = accum;
+    d.cgrid = cgrid;
+    d.rgrid = rgrid;
+    d.bmod = bmod;
+    d.ktab = ktab;
+    d.tw = tw;
+    d.acc = acc;
+    d.ev = ev;
+    d.tx_rows = tx_rows; d.tx_y = tx_y; d.tx_z = tx_z;
+    return d;
+  }
+};
+
+}  // namespace
+
+struct pme_recip {
+  int fft_type = PME_FFT_BOX;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  SystemState st;
+  char* d_block = nullptr;
+  unsigned int* d_bar = nullptr;
+  int* d_status = nullptr;
+  bool accum_dirty = false;
+  size_t max_smem = 0;
+  unsigned int spin_limit = 1u << 22;
+  int inject = 0;
+  unsigned long long* trace = nullptr;
+  int trace_ctas = 0;
+};
+
+struct pme_batch {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::vector<SystemState> st;
+  std::vector<SysDesc> desc;
+  SysDesc* d_desc = nullptr;
+  int* d_prefix = nullptr;
+  int total[kPhases] = {0};
+  char* d_block = nullptr;
+  unsigned int* d_bar = nullptr;
+  int* d_status = nullptr;
+  size_t smem = 0;
+  int grid = 0;
+  unsigned int spin_limit = 1u << 22;
+  size_t bytes = 0;
+  unsigned long long* trace = nullptr;
+  int trace_ctas = 0;
+};
+
+namespace {
+
+void release(pme_recip* h) {
+  if (!h) return;
+  cudaFree(h->d_block);
+  cudaFree(h->d_bar);
+  delete h;
+}
+
+int handle_ok(const pme_recip* h) { return h ? PME_OK : fail(PME_EINVAL, "handle is NULL"); }
+
+// 3 doubles of the reciprocal diagonal
+void diag3(const double* recip, double* r3) {
+  r3[0] = recip[0];
+  r3[1] = recip[4];
+  r3[2] = recip[8];
+}
+
+int launch_fused_single(pme_recip* h, const SysDesc& d) {
+  FusedArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.table = nullptr;
+  a.single = d;
+  a.nsys = 1;
+  a.prefix = nullptr;
+  fused_tile_counts(d, a.total);
+  a.bar = h->d_bar;
+  a.status = h->d_status;
+  a.spin_limit = h->spin_limit;
+  a.inject = h->inject;
+  a.trace = h->trace;
+  a.trace_ctas = h->trace_ctas;
+  const size_t smem = fused_smem_bytes(d);
+  int grid = 0;
+  cudaError_t e = fused_max_grid(smem, &grid);
+  if (e != cudaSuccess) return cuda_fail(e, "fused: occupancy");
+  if (grid < 1) return fail(PME_EUNSUPPORTED, "fused kernel does not fit on an SM");
+  int most = 1;
+  for (int p = 0; p < kPhases; p++) most = std::max(most, a.total[p]);
+  grid = std::max(1, std::min(grid, most));
+  e = fused_launch(a, grid, smem, h->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "fused eval launch");
   return PME_OK;
 }
 
@@ -275,78 +374,32 @@ int pme_create(int nfftx, int nffty, int nfftz, int order, int fft_type, int nno
     return fail(PME_EUNSUPPORTED, "multi-node grid decomposition is not supported (nnode must be 1)");
   if (fft_type != PME_FFT_COLUMN && fft_type != PME_FFT_SLAB && fft_type != PME_FFT_BOX)
     return fail(PME_EINVAL, "invalid fft_type");
-  if (!valid_order(order)) return fail(PME_EINVAL, "order must be 4, 6 or 8");
-  const int n3[3] = {nfftx, nffty, nfftz};
-  for (int d = 0; d < 3; d++) {
-    if (n3[d] < order || n3[d] > kMaxFftLen)
-      return fail(PME_EINVAL, "grid lengths must be in [order, 512]");
-  }
+  int rc = check_grid(nfftx, nffty, nfftz, order);
+  if (rc) return rc;
   pme_recip* h = new (std::nothrow) pme_recip();
   if (!h) return fail(PME_ENOMEM, "host allocation failed");
-  std::memset(h, 0, sizeof(*h));
-  h->nx = nfftx; h->ny = nffty; h->nz = nfftz;
-  h->order = order;
   h->fft_type = fft_type;
   h->stream = (cudaStream_t)stream;
-  if (!factorize(nfftx, h->px) || !factorize(nffty, h->py) || !factorize(nfftz, h->pz)) {
-    delete h;
-    return fail(PME_EUNSUPPORTED, "grid lengths must factor into 2, 3 and 5");
-  }
   cudaError_t e = cudaGetDevice(&h->device);
   if (e != cudaSuccess) { delete h; return cuda_fail(e, "cudaGetDevice"); }
-  e = configure_kernels();
+  e = configure_kernels(&h->max_smem);
   if (e != cudaSuccess) { delete h; return cuda_fail(e, "configure kernels"); }
-
-  h->px.tw_off = 0;
-  h->py.tw_off = nfftx;
-  h->pz.tw_off = nfftx + nffty;
-  const int hx = nfftx / 2 + 1;
-  h->tile_x = pick_tiling_rows(nfftx);
-  h->tile_y = pick_tiling_cols(hx, nffty);
-  h->tile_z = pick_tiling_cols(hx, nfftz);
-
-  const size_t G = (size_t)nfftx * nffty * nfftz;
-  const size_t H = (size_t)hx * nffty * nfftz;
-  Geom g0 = make_geom(h, nullptr);
-  const int zblocks = c2c_num_blocks(g0, 2, h->tile_z);
-  h->max_blocks = zblocks > 1024 ? zblocks : 1024;
-
-  bool ok = cudaMalloc(&h->d_accum, G * sizeof(long long)) == cudaSuccess &&
-            cudaMalloc(&h->d_cgrid, H * sizeof(float2)) == cudaSuccess &&
-            cudaMalloc(&h->d_rgrid, G * sizeof(float)) == cudaSuccess &&
-            cudaMalloc(&h->d_tw, (size_t)(nfftx + nffty + nfftz) * sizeof(float2)) == cudaSuccess &&
-            cudaMalloc(&h->d_bmod, (size_t)(nfftx + nffty + nfftz) * sizeof(float)) == cudaSuccess &&
-            cudaMalloc(&h->d_ev, PME_EV_COUNT * sizeof(double)) == cudaSuccess &&
-            cudaMalloc(&h->d_partials, (size_t)h->max_blocks * 8 * sizeof(double)) == cudaSuccess &&
-            cudaMalloc(&h->d_ticket, kNumSites * sizeof(unsigned int)) == cudaSuccess;
-  if (!ok) {
+  h->st.setup(nfftx, nffty, nfftz, order);
+  const size_t bytes = SystemState::bytes(nfftx, nffty, nfftz);
+  if (cudaMalloc(&h->d_block, bytes) != cudaSuccess ||
+      cudaMalloc(&h->d_bar, 4 * sizeof(unsigned int)) != cudaSuccess) {
     cudaGetLastError();
     release(h);
     return fail(PME_ENOMEM, "device allocation failed");
   }
-  // twiddles W_n^k = exp(-2 pi i k/n), FP64 -> FP32
-  std::vector<float2> tw;
-  for (int d = 0; d < 3; d++) {
-    const int n = n3[d];
-    for (int k = 0; k < n; k++) {
-      const double a = -2.0 * kPi * (double)k / (double)n;
-      tw.push_back(make_float2((float)std::cos(a), (float)std::sin(a)));
-    }
-  }
-  e = cudaMemcpy(h->d_tw, tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemset(h->d_ev, 0, PME_EV_COUNT * sizeof(double));
-  if (e == cudaSuccess) e = cudaMemset(h->d_ticket, 0, kNumSites * sizeof(unsigned int));
-  if (e == cudaSuccess) e = cudaMemset(h->d_accum, 0, G * sizeof(long long));
-  if (e == cudaSuccess) e = cudaMemset(h->d_cgrid, 0, H * sizeof(float2));
-  if (e == cudaSuccess) e = cudaMemset(h->d_rgrid, 0, G * sizeof(float));
+  h->d_status = (int*)(h->d_bar + 2);
+  h->st.carve(h->d_block);
+  e = cudaMemset(h->d_block, 0, bytes);
+  if (e == cudaSuccess) e = cudaMemset(h->d_bar, 0, 4 * sizeof(unsigned int));
+  if (e == cudaSuccess) e = h->st.upload_tables();
   if (e != cudaSuccess) {
     release(h);
     return cuda_fail(e, "pme_create: initialise buffers");
-  }
-  int rc = upload_moduli(h);
-  if (rc != PME_OK) {
-    release(h);
-    return rc;
   }
   *out = h;
   return PME_OK;
@@ -360,194 +413,180 @@ int pme_destroy(pme_recip* h) {
 }
 
 int pme_set_stream(pme_recip* h, void* stream) {
-  if (!h) return fail(PME_EINVAL, "handle is NULL");
+  if (int rc = handle_ok(h)) return rc;
   h->stream = (cudaStream_t)stream;
   return PME_OK;
 }
 
 int pme_set_order(pme_recip* h, int order) {
-  if (!h) return fail(PME_EINVAL, "handle is NULL");
-  if (!valid_order(order)) return fail(PME_EINVAL, "order must be 4, 6 or 8");
-  if (h->nx < order || h->ny < order || h->nz < order)
-    return fail(PME_EINVAL, "grid lengths must be >= order");
+  if (int rc = handle_ok(h)) return rc;
+  if (int rc = check_grid(h->st.nx, h->st.ny, h->st.nz, order)) return rc;
   DeviceGuard dg(h->device);
-  // moduli are uploaded synchronously after the stream's pending work
-  cudaError_t e = cudaStreamSynchronize(h->stream);
+  cudaError_t e = cudaStreamSynchronize(h->stream);   // tables are replaced synchronously
   if (e != cudaSuccess) return cuda_fail(e, "set_order");
-  h->order = order;
-  return upload_moduli(h);
+  h->st.order = order;
+  e = h->st.upload_tables();
+  if (e != cudaSuccess) return cuda_fail(e, "set_order: upload moduli");
+  return PME_OK;
 }
 
 int pme_get_nfft(const pme_recip* h, int* nx, int* ny, int* nz) {
-  if (!h) return fail(PME_EINVAL, "handle is NULL");
-  if (nx) *nx = h->nx;
-  if (ny) *ny = h->ny;
-  if (nz) *nz = h->nz;
+  if (int rc = handle_ok(h)) return rc;
+  if (nx) *nx = h->st.nx;
+  if (ny) *ny = h->st.ny;
+  if (nz) *nz = h->st.nz;
   return PME_OK;
 }
 
 int pme_get_order(const pme_recip* h, int* order) {
   if (!h || !order) return fail(PME_EINVAL, "NULL argument");
-  *order = h->order;
+  *order = h->st.order;
   return PME_OK;
 }
 
 int pme_print_info(const pme_recip* h) {
-  if (!h) return fail(PME_EINVAL, "handle is NULL");
+  if (int rc = handle_ok(h)) return rc;
+  const SystemState& s = h->st;
   const char* ft = h->fft_type == PME_FFT_COLUMN ? "COLUMN" : (h->fft_type == PME_FFT_SLAB ? "SLAB" : "BOX");
   std::printf("fft_type = %s computed using the built-in sm_100a 2/3/5-radix FFT\n", ft);
-  std::printf("order = %d\n", h->order);
-  std::printf("nfftx, nffty, nfftz = %d %d %d\n", h->nx, h->ny, h->nz);
-  std::printf("x0...x1   = 0 ... %d\ny0...y1   = 0 ... %d\nz0...z1   = 0 ... %d\n", h->nx - 1,
-              h->ny - 1, h->nz - 1);
-  std::printf("xsize, ysize, zsize = %d %d %d\n", h->nx, h->ny, h->nz);
-  std::printf("data_size = %d\n", 2 * (h->nx / 2 + 1) * h->ny * h->nz);
-  std::printf("tiles: x %d, y %d, z %d lines per CTA\n", h->tile_x.tx, h->tile_y.tx, h->tile_z.tx);
+  std::printf("order = %d\n", s.order);
+  std::printf("nfftx, nffty, nfftz = %d %d %d\n", s.nx, s.ny, s.nz);
+  std::printf("x0...x1   = 0 ... %d\ny0...y1   = 0 ... %d\nz0...z1   = 0 ... %d\n", s.nx - 1, s.ny - 1,
+              s.nz - 1);
+  std::printf("xsize, ysize, zsize = %d %d %d\n", s.nx, s.ny, s.nz);
+  std::printf("data_size = %d\n", 2 * (s.nx / 2 + 1) * s.ny * s.nz);
+  std::printf("tiles: x %d rows, y %d, z %d columns per CTA\n", s.tx_rows, s.tx_y, s.tx_z);
   std::fflush(stdout);
   return PME_OK;
 }
 
 int pme_spread_charge(pme_recip* h, const void* xyzq, int ncoord, const double* recip) {
-  if (!h) return fail(PME_EINVAL, "handle is NULL");
+  if (int rc = handle_ok(h)) return rc;
   if (ncoord < 0 || (ncoord > 0 && !xyzq)) return fail(PME_EINVAL, "bad xyzq/ncoord");
-  int rc = check_recip(recip);
-  if (rc) return rc;
+  if (int rc = check_recip(recip)) return rc;
   DeviceGuard dg(h->device);
-  return enqueue_spread(h, xyzq, ncoord, make_geom(h, recip));
-}
-
-int pme_r2c_fft(pme_recip* h) {
-  if (!h) return fail(PME_EINVAL, "handle is NULL");
-  DeviceGuard dg(h->device);
-  Geom g = make_geom(h, nullptr);
-  int rc = enqueue_r2c(h, g);
-  if (rc) return rc;
-  cudaError_t e =
-      launch_c2c(h->d_cgrid, g, 2, 0, h->pz, h->d_tw, h->tile_z, nullptr, scratch(h), 0, h->stream);
-  if (e != cudaSuccess) return cuda_fail(e, "r2c_fft: z pass");
+  double r3[3];
+  diag3(recip, r3);
+  cudaError_t e = cudaMemsetAsync(h->st.accum, 0, h->st.G() * 8, h->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "spread_charge: clear grid");
+  e = staged_spread(h->st.desc(r3, 0.0, xyzq, ncoord, nullptr, 0, 0, 0, 0), h->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "spread_charge");
+  h->accum_dirty = true;
   return PME_OK;
 }
 
-int pme_scalar_sum(pme_recip* h, const double* recip, double kappa, int calc_energy,
-                   int calc_virial) {
-  if (!h) return fail(PME_EINVAL, "handle is NULL");
-  int rc = check_recip(recip);
-  if (rc) return rc;
+int pme_r2c_fft(pme_recip* h) {
+  if (int rc = handle_ok(h)) return rc;
+  DeviceGuard dg(h->device);
+  cudaError_t e = staged_r2c(h->st.desc(nullptr, 0.0, nullptr, 0, nullptr, 0, 0, 0, 0), true, h->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "r2c_fft");
+  h->accum_dirty = false;
+  return PME_OK;
+}
+
+int pme_scalar_sum(pme_recip* h, const double* recip, double kappa, int calc_energy, int calc_virial) {
+  if (int rc = handle_ok(h)) return rc;
+  if (int rc = check_recip(recip)) return rc;
   if (!(kappa > 0.0) || !std::isfinite(kappa)) return fail(PME_EINVAL, "kappa must be positive");
   DeviceGuard dg(h->device);
-  Geom g = make_geom(h, recip);
-  SolveParams sp = solve_params(h, recip, kappa, (calc_energy || calc_virial) ? 1 : 0);
-  cudaError_t e =
-      launch_c2c(h->d_cgrid, g, 2, 3, h->pz, h->d_tw, h->tile_z, &sp, scratch(h), kSiteSolve, h->stream);
+  double r3[3];
+  diag3(recip, r3);
+  const int ev = (calc_energy || calc_virial) ? 1 : 0;
+  cudaError_t e = staged_solve(h->st.desc(r3, kappa, nullptr, 0, nullptr, 0, 0, ev, 0), h->stream);
   if (e != cudaSuccess) return cuda_fail(e, "scalar_sum");
   return PME_OK;
 }
 
 int pme_c2r_fft(pme_recip* h) {
-  if (!h) return fail(PME_EINVAL, "handle is NULL");
+  if (int rc = handle_ok(h)) return rc;
   DeviceGuard dg(h->device);
-  Geom g = make_geom(h, nullptr);
-  cudaError_t e =
-      launch_c2c(h->d_cgrid, g, 2, 1, h->pz, h->d_tw, h->tile_z, nullptr, scratch(h), 0, h->stream);
-  if (e != cudaSuccess) return cuda_fail(e, "c2r_fft: z pass");
-  return enqueue_c2r_tail(h, g);
+  cudaError_t e = staged_c2r(h->st.desc(nullptr, 0.0, nullptr, 0, nullptr, 0, 0, 0, 0), h->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "c2r_fft");
+  return PME_OK;
 }
 
 int pme_gather_force(pme_recip* h, const void* xyzq, int ncoord, const double* recip, int stride,
                      int kind, void* force) {
-  if (!h) return fail(PME_EINVAL, "handle is NULL");
+  if (int rc = handle_ok(h)) return rc;
   if (ncoord < 0 || (ncoord > 0 && !xyzq)) return fail(PME_EINVAL, "bad xyzq/ncoord");
-  int rc = check_recip(recip);
-  if (rc) return rc;
-  rc = check_force_args(ncoord, stride, kind, force);
-  if (rc) return rc;
+  if (int rc = check_recip(recip)) return rc;
+  if (int rc = check_force_args(ncoord, stride, kind, force)) return rc;
   DeviceGuard dg(h->device);
-  cudaError_t e = launch_gather((const float4*)xyzq, ncoord, make_geom(h, recip), h->order,
-                                h->d_rgrid, kind, stride, force, h->stream);
+  double r3[3];
+  diag3(recip, r3);
+  cudaError_t e = staged_gather(h->st.desc(r3, 0.0, xyzq, ncoord, force, kind, stride, 0, 0), h->stream);
   if (e != cudaSuccess) return cuda_fail(e, "gather_force");
   return PME_OK;
 }
 
 int pme_calc_self_energy(pme_recip* h, const void* xyzq, int ncoord, double kappa) {
-  if (!h) return fail(PME_EINVAL, "handle is NULL");
+  if (int rc = handle_ok(h)) return rc;
   if (ncoord < 0 || (ncoord > 0 && !xyzq)) return fail(PME_EINVAL, "bad xyzq/ncoord");
   if (!std::isfinite(kappa)) return fail(PME_EINVAL, "kappa must be finite");
   DeviceGuard dg(h->device);
-  cudaError_t e = launch_self_energy((const float4*)xyzq, ncoord, kappa, h->d_ev, scratch(h),
-                                     kSiteSelf, h->stream);
+  cudaError_t e = staged_self(h->st.desc(nullptr, kappa, xyzq, ncoord, nullptr, 0, 0, 0, 1), h->stream);
   if (e != cudaSuccess) return cuda_fail(e, "calc_self_energy");
   return PME_OK;
 }
 
 int pme_clear_energy_virial(pme_recip* h) {
-  if (!h) return fail(PME_EINVAL, "handle is NULL");
+  if (int rc = handle_ok(h)) return rc;
   DeviceGuard dg(h->device);
-  cudaError_t e = cudaMemsetAsync(h->d_ev, 0, PME_EV_COUNT * sizeof(double), h->stream);
+  cudaError_t e = cudaMemsetAsync(h->st.ev, 0, kEvCount * sizeof(double), h->stream);
   if (e != cudaSuccess) return cuda_fail(e, "clear_energy_virial");
   return PME_OK;
 }
 
-int pme_get_energy_virial(pme_recip* h, double* energy_recip, double* energy_self,
-                          double* virial9) {
-  if (!h) return fail(PME_EINVAL, "handle is NULL");
+int pme_get_energy_virial(pme_recip* h, double* energy_recip, double* energy_self, double* virial9) {
+  if (int rc = handle_ok(h)) return rc;
   DeviceGuard dg(h->device);
-  double buf[PME_EV_COUNT];
-  cudaError_t e = cudaMemcpyAsync(buf, h->d_ev, sizeof(buf), cudaMemcpyDeviceToHost, h->stream);
+  double buf[kEvCount];
+  int status = 0;
+  cudaError_t e = cudaMemcpyAsync(buf, h->st.ev, sizeof(buf), cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&status, h->d_status, sizeof(int), cudaMemcpyDeviceToHost, h->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
   if (e != cudaSuccess) return cuda_fail(e, "get_energy_virial");
-  if (energy_recip) *energy_recip = buf[PME_EV_RECIP];
-  if (energy_self) *energy_self = buf[PME_EV_SELF];
-  if (virial9) for (int i = 0; i < 9; i++) virial9[i] = buf[PME_EV_VIRIAL + i];
+  if (energy_recip) *energy_recip = buf[kEvRecip];
+  if (energy_self) *energy_self = buf[kEvSelf];
+  if (virial9) for (int i = 0; i < 9; i++) virial9[i] = buf[kEvVirial + i];
+  if (status != kStatusOk)
+    return fail(PME_ETIMEOUT, "a grid barrier of the fused evaluation timed out; results are incomplete");
   return PME_OK;
 }
 
 int pme_copy_energy_virial_async(pme_recip* h, double* dst) {
   if (!h || !dst) return fail(PME_EINVAL, "NULL argument");
   DeviceGuard dg(h->device);
-  cudaError_t e = cudaMemcpyAsync(dst, h->d_ev, PME_EV_COUNT * sizeof(double), cudaMemcpyDefault,
-                                  h->stream);
+  cudaError_t e = cudaMemcpyAsync(dst, h->st.ev, kEvCount * sizeof(double), cudaMemcpyDefault, h->stream);
   if (e != cudaSuccess) return cuda_fail(e, "copy_energy_virial_async");
   return PME_OK;
 }
 
 int pme_energy_virial_device_ptr(pme_recip* h, double** dev_ptr) {
   if (!h || !dev_ptr) return fail(PME_EINVAL, "NULL argument");
-  *dev_ptr = h->d_ev;
+  *dev_ptr = h->st.ev;
   return PME_OK;
 }
 
-int pme_eval_ortho(pme_recip* h, double inv_boxx, double inv_boxy, double inv_boxz,
-                   const void* xyzq, int ncoord, double kappa, int calc_energy, int calc_virial,
-                   int kind, void* force, int stride) {
-  if (!h) return fail(PME_EINVAL, "handle is NULL");
+int pme_eval_ortho(pme_recip* h, double inv_boxx, double inv_boxy, double inv_boxz, const void* xyzq,
+                   int ncoord, double kappa, int calc_energy, int calc_virial, int kind, void* force,
+                   int stride) {
+  if (int rc = handle_ok(h)) return rc;
   if (ncoord < 0 || (ncoord > 0 && !xyzq)) return fail(PME_EINVAL, "bad xyzq/ncoord");
-  double recip[9] = {inv_boxx, 0, 0, 0, inv_boxy, 0, 0, 0, inv_boxz};
-  int rc = check_recip(recip);
-  if (rc) return rc;
+  const double recip[9] = {inv_boxx, 0, 0, 0, inv_boxy, 0, 0, 0, inv_boxz};
+  if (int rc = check_recip(recip)) return rc;
   if (!(kappa > 0.0) || !std::isfinite(kappa)) return fail(PME_EINVAL, "kappa must be positive");
-  rc = check_force_args(ncoord, stride, kind, force);
-  if (rc) return rc;
+  if (int rc = check_force_args(ncoord, stride, kind, force)) return rc;
   DeviceGuard dg(h->device);
-  Geom g = make_geom(h, recip);
-  rc = enqueue_spread(h, xyzq, ncoord, g);
-  if (rc) return rc;
-  rc = enqueue_r2c(h, g);
-  if (rc) return rc;
-  SolveParams sp = solve_params(h, recip, kappa, (calc_energy || calc_virial) ? 1 : 0);
-  cudaError_t e =
-      launch_c2c(h->d_cgrid, g, 2, 2, h->pz, h->d_tw, h->tile_z, &sp, scratch(h), kSiteSolve, h->stream);
-  if (e != cudaSuccess) return cuda_fail(e, "eval: z pass + solve");
-  rc = enqueue_c2r_tail(h, g);
-  if (rc) return rc;
-  e = launch_gather((const float4*)xyzq, ncoord, g, h->order, h->d_rgrid, kind, stride, force,
-                    h->stream);
-  if (e != cudaSuccess) return cuda_fail(e, "eval: gather");
-  if (calc_energy) {
-    e = launch_self_energy((const float4*)xyzq, ncoord, kappa, h->d_ev, scratch(h), kSiteSelf,
-                           h->stream);
-    if (e != cudaSuccess) return cuda_fail(e, "eval: self energy");
+  if (h->accum_dirty) {   // a staged spread_charge is pending: start from an empty grid
+    cudaError_t e = cudaMemsetAsync(h->st.accum, 0, h->st.G() * 8, h->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "eval: clear grid");
+    h->accum_dirty = false;
   }
-  return PME_OK;
+  const double r3[3] = {inv_boxx, inv_boxy, inv_boxz};
+  const int ev = (calc_energy || calc_virial) ? 1 : 0;
+  SysDesc d = h->st.desc(r3, kappa, xyzq, ncoord, force, kind, stride, ev, calc_energy ? 1 : 0);
+  return launch_fused_single(h, d);
 }
 
 static int copy_back(pme_recip* h, void* dst, const void* src, size_t bytes, const char* what) {
@@ -560,46 +599,84 @@ static int copy_back(pme_recip* h, void* dst, const void* src, size_t bytes, con
 }
 
 int pme_copy_charge_grid_fixed(pme_recip* h, long long* host_out) {
-  if (!h) return fail(PME_EINVAL, "handle is NULL");
-  const size_t G = (size_t)h->nx * h->ny * h->nz;
-  return copy_back(h, host_out, h->d_accum, G * sizeof(long long), "copy_charge_grid_fixed");
+  if (int rc = handle_ok(h)) return rc;
+  return copy_back(h, host_out, h->st.accum, h->st.G() * 8, "copy_charge_grid_fixed");
 }
 
 int pme_copy_charge_grid(pme_recip* h, float* host_out) {
   if (!h || !host_out) return fail(PME_EINVAL, "NULL argument");
-  const size_t G = (size_t)h->nx * h->ny * h->nz;
-  std::vector<long long> tmp(G);
-  int rc = copy_back(h, tmp.data(), h->d_accum, G * sizeof(long long), "copy_charge_grid");
+  std::vector<long long> tmp(h->st.G());
+  int rc = copy_back(h, tmp.data(), h->st.accum, h->st.G() * 8, "copy_charge_grid");
   if (rc) return rc;
-  for (size_t i = 0; i < G; i++) host_out[i] = (float)((double)tmp[i] * kInvFixedScale);
+  for (size_t i = 0; i < tmp.size(); i++) host_out[i] = (float)((double)tmp[i] * kInvFixedScale);
   return PME_OK;
 }
 
 int pme_copy_fft_grid(pme_recip* h, float* host_out) {
-  if (!h) return fail(PME_EINVAL, "handle is NULL");
-  const size_t H = (size_t)(h->nx / 2 + 1) * h->ny * h->nz;
-  return copy_back(h, host_out, h->d_cgrid, H * sizeof(float2), "copy_fft_grid");
+  if (int rc = handle_ok(h)) return rc;
+  return copy_back(h, host_out, h->st.cgrid, h->st.H() * 8, "copy_fft_grid");
 }
 
 int pme_copy_solved_grid(pme_recip* h, float* host_out) {
-  if (!h) return fail(PME_EINVAL, "handle is NULL");
-  const size_t G = (size_t)h->nx * h->ny * h->nz;
-  return copy_back(h, host_out, h->d_rgrid, G * sizeof(float), "copy_solved_grid");
+  if (int rc = handle_ok(h)) return rc;
+  return copy_back(h, host_out, h->st.rgrid, h->st.G() * 4, "copy_solved_grid");
 }
 
 int pme_load_charge_grid(pme_recip* h, const float* host_in) {
   if (!h || !host_in) return fail(PME_EINVAL, "NULL argument");
-  const size_t G = (size_t)h->nx * h->ny * h->nz;
-  std::vector<long long> tmp(G);
-  for (size_t i = 0; i < G; i++) {
+  std::vector<long long> tmp(h->st.G());
+  for (size_t i = 0; i < tmp.size(); i++) {
     const double v = (double)host_in[i] * 1099511627776.0;
     if (!(std::fabs(v) < 9.0e18)) return fail(PME_EINVAL, "grid value out of fixed-point range");
     tmp[i] = std::llrint(v);
   }
   DeviceGuard dg(h->device);
   cudaError_t e = cudaStreamSynchronize(h->stream);
-  if (e == cudaSuccess) e = cudaMemcpy(h->d_accum, tmp.data(), G * sizeof(long long), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(h->st.accum, tmp.data(), tmp.size() * 8, cudaMemcpyHostToDevice);
   if (e != cudaSuccess) return cuda_fail(e, "load_charge_grid");
+  h->accum_dirty = true;
+  return PME_OK;
+}
+
+int pme_get_status(pme_recip* h, int* device_status) {
+  if (int rc = handle_ok(h)) return rc;
+  DeviceGuard dg(h->device);
+  int status = 0;
+  cudaError_t e = cudaMemcpyAsync(&status, h->d_status, sizeof(int), cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "get_status");
+  if (device_status) *device_status = status;
+  if (status != kStatusOk) {
+    // clear the sticky status, the barrier words, the accumulation grid and the accumulators
+    // (an interrupted evaluation leaves them partly filled) so the handle is usable again
+    e = cudaMemsetAsync(h->d_bar, 0, 4 * sizeof(unsigned int), h->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(h->st.accum, 0, h->st.G() * 8, h->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(h->st.acc, 0, kAccCount * sizeof(long long), h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "get_status: reset");
+    return fail(PME_ETIMEOUT, "a grid barrier of the fused evaluation timed out");
+  }
+  return PME_OK;
+}
+
+int pme_set_barrier_spin_limit(pme_recip* h, unsigned int polls) {
+  if (int rc = handle_ok(h)) return rc;
+  h->spin_limit = polls == 0 ? 1u : polls;
+  return PME_OK;
+}
+
+int pme_set_fault_injection(pme_recip* h, int what) {
+  if (int rc = handle_ok(h)) return rc;
+  if (what != PME_INJECT_NONE && what != PME_INJECT_SKIP_BARRIER) return fail(PME_EINVAL, "unknown injection");
+  h->inject = what;
+  return PME_OK;
+}
+
+int pme_set_trace(pme_recip* h, unsigned long long* dev_buf, int max_ctas) {
+  if (int rc = handle_ok(h)) return rc;
+  if (dev_buf && max_ctas <= 0) return fail(PME_EINVAL, "max_ctas must be positive");
+  h->trace = dev_buf;
+  h->trace_ctas = dev_buf ? max_ctas : 0;
   return PME_OK;
 }
 
@@ -618,6 +695,198 @@ const char* pme_status_string(int status) {
   }
 }
 
-int pme_version(void) { return 100; }
+int pme_version(void) { return 200; }
+
+// ---------------------------------------------------------------------------------------------
+// Batches: many independent systems, one persistent launch per evaluation.
+// ---------------------------------------------------------------------------------------------
+int pme_batch_commit(pme_batch* b);
+
+int pme_batch_destroy(pme_batch* b) {
+  if (!b) return PME_OK;
+  DeviceGuard dg(b->device);
+  cudaFree(b->d_block);
+  cudaFree(b->d_desc);
+  cudaFree(b->d_bar);
+  delete b;
+  return PME_OK;
+}
+
+int pme_batch_create(const pme_system_desc* systems, int nsys, void* stream, pme_batch** out) {
+  if (!out) return fail(PME_EINVAL, "out is NULL");
+  *out = nullptr;
+  if (!systems || nsys <= 0) return fail(PME_EINVAL, "need at least one system");
+  for (int i = 0; i < nsys; i++) {
+    const pme_system_desc& s = systems[i];
+    if (int rc = check_grid(s.nfftx, s.nffty, s.nfftz, s.order)) return rc;
+    if (s.natom < 0 || (s.natom > 0 && !s.xyzq)) return fail(PME_EINVAL, "bad xyzq/natom in a batch system");
+    if (!(s.box[0] > 0 && s.box[1] > 0 && s.box[2] > 0) || !(s.kappa > 0))
+      return fail(PME_EINVAL, "box edges and kappa must be positive");
+    if (int rc = check_force_args(s.natom, s.stride, s.force_kind, s.force)) return rc;
+  }
+  pme_batch* b = new (std::nothrow) pme_batch();
+  if (!b) return fail(PME_ENOMEM, "host allocation failed");
+  b->stream = (cudaStream_t)stream;
+  cudaError_t e = cudaGetDevice(&b->device);
+  size_t max_smem = 0;
+  if (e == cudaSuccess) e = configure_kernels(&max_smem);
+  if (e != cudaSuccess) { delete b; return cuda_fail(e, "batch: configure kernels"); }
+  b->st.resize(nsys);
+  std::vector<size_t> off(nsys);
+  size_t total = 0;
+  for (int i = 0; i < nsys; i++) {
+    b->st[i].setup(systems[i].nfftx, systems[i].nffty, systems[i].nfftz, systems[i].order);
+    off[i] = total;
+    total += SystemState::bytes(systems[i].nfftx, systems[i].nffty, systems[i].nfftz);
+  }
+  b->bytes = total;
+  const size_t table_bytes = align256(sizeof(SysDesc) * nsys) + align256(sizeof(int) * kPhases * (nsys + 1));
+  if (cudaMalloc(&b->d_block, total) != cudaSuccess || cudaMalloc(&b->d_desc, table_bytes) != cudaSuccess ||
+      cudaMalloc(&b->d_bar, 4 * sizeof(unsigned int)) != cudaSuccess) {
+    cudaGetLastError();
+    pme_batch_destroy(b);
+    return fail(PME_ENOMEM, "batch: device allocation failed");
+  }
+  b->d_prefix = (int*)((char*)b->d_desc + align256(sizeof(SysDesc) * nsys));
+  b->d_status = (int*)(b->d_bar + 2);
+  e = cudaMemset(b->d_block, 0, total);
+  if (e == cudaSuccess) e = cudaMemset(b->d_bar, 0, 4 * sizeof(unsigned int));
+  for (int i = 0; i < nsys && e == cudaSuccess; i++) {
+    b->st[i].carve(b->d_block + off[i]);
+    e = b->st[i].upload_tables();
+  }
+  if (e != cudaSuccess) {
+    pme_batch_destroy(b);
+    return cuda_fail(e, "batch: initialise buffers");
+  }
+  b->desc.resize(nsys);
+  for (int i = 0; i < nsys; i++) {
+    const pme_system_desc& s = systems[i];
+    const double r3[3] = {1.0 / s.box[0], 1.0 / s.box[1], 1.0 / s.box[2]};
+    const int ev = (s.calc_energy || s.calc_virial) ? 1 : 0;
+    b->desc[i] = b->st[i].desc(r3, s.kappa, s.xyzq, s.natom, s.force, s.force_kind, s.stride, ev,
+                               s.calc_energy ? 1 : 0);
+  }
+  int rc = pme_batch_commit(b);
+  if (rc) {
+    pme_batch_destroy(b);
+    return rc;
+  }
+  *out = b;
+  return PME_OK;
+}
+
+int pme_batch_commit(pme_batch* b) {
+  if (!b) return fail(PME_EINVAL, "batch is NULL");
+  DeviceGuard dg(b->device);
+  const int nsys = (int)b->desc.size();
+  std::vector<int> prefix((size_t)kPhases * (nsys + 1), 0);
+  size_t smem = 0;
+  for (int i = 0; i < nsys; i++) {
+    int cnt[kPhases];
+    fused_tile_counts(b->desc[i], cnt);
+    for (int p = 0; p < kPhases; p++)
+      prefix[(size_t)p * (nsys + 1) + i + 1] = prefix[(size_t)p * (nsys + 1) + i] + cnt[p];
+    smem = std::max(smem, fused_smem_bytes(b->desc[i]));
+  }
+  for (int p = 0; p < kPhases; p++) b->total[p] = prefix[(size_t)p * (nsys + 1) + nsys];
+  cudaError_t e = cudaStreamSynchronize(b->stream);
+  if (e == cudaSuccess) e = cudaMemcpy(b->d_desc, b->desc.data(), sizeof(SysDesc) * nsys, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(b->d_prefix, prefix.data(), prefix.size() * sizeof(int), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return cuda_fail(e, "batch: upload descriptors");
+  b->smem = smem;
+  int grid = 0;
+  e = fused_max_grid(smem, &grid);
+  if (e != cudaSuccess) return cuda_fail(e, "batch: occupancy");
+  if (grid < 1) return fail(PME_EUNSUPPORTED, "batch: kernel does not fit on an SM");
+  int most = 1;
+  for (int p = 0; p < kPhases; p++) most = std::max(most, b->total[p]);
+  b->grid = std::min(grid, most);
+  return PME_OK;
+}
+
+int pme_batch_set_system(pme_batch* b, int sys, const double* box3, const void* xyzq, void* force) {
+  if (!b || sys < 0 || sys >= (int)b->desc.size()) return fail(PME_EINVAL, "bad batch or system index");
+  SysDesc& d = b->desc[sys];
+  if (box3) {
+    if (!(box3[0] > 0 && box3[1] > 0 && box3[2] > 0)) return fail(PME_EINVAL, "box edges must be positive");
+    const double r3[3] = {1.0 / box3[0], 1.0 / box3[1], 1.0 / box3[2]};
+    const double kappa = kPi / std::sqrt(d.fac);
+    d = b->st[sys].desc(r3, kappa, d.xyzq, d.natom, d.force, d.force_kind, d.stride, d.calc_ev, d.calc_self);
+  }
+  if (xyzq) d.xyzq = (const float4*)xyzq;
+  if (force) d.force = force;
+  return PME_OK;
+}
+
+int pme_batch_eval(pme_batch* b) {
+  if (!b) return fail(PME_EINVAL, "batch is NULL");
+  DeviceGuard dg(b->device);
+  FusedArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.table = b->d_desc;
+  a.nsys = (int)b->desc.size();
+  a.prefix = b->d_prefix;
+  for (int p = 0; p < kPhases; p++) a.total[p] = b->total[p];
+  a.bar = b->d_bar;
+  a.status = b->d_status;
+  a.spin_limit = b->spin_limit;
+  a.trace = b->trace;
+  a.trace_ctas = b->trace_ctas;
+  cudaError_t e = fused_launch(a, b->grid, b->smem, b->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "batch eval launch");
+  return PME_OK;
+}
+
+int pme_batch_clear_energy_virial(pme_batch* b) {
+  if (!b) return fail(PME_EINVAL, "batch is NULL");
+  DeviceGuard dg(b->device);
+  for (size_t i = 0; i < b->st.size(); i++) {
+    cudaError_t e = cudaMemsetAsync(b->st[i].ev, 0, kEvCount * sizeof(double), b->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "batch clear");
+  }
+  return PME_OK;
+}
+
+int pme_batch_get_energy_virial(pme_batch* b, double* out) {
+  if (!b || !out) return fail(PME_EINVAL, "NULL argument");
+  DeviceGuard dg(b->device);
+  int status = 0;
+  cudaError_t e = cudaSuccess;
+  for (size_t i = 0; i < b->st.size() && e == cudaSuccess; i++)
+    e = cudaMemcpyAsync(out + i * kEvCount, b->st[i].ev, kEvCount * sizeof(double), cudaMemcpyDeviceToHost,
+                        b->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&status, b->d_status, sizeof(int), cudaMemcpyDeviceToHost, b->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "batch get energy/virial");
+  if (status != kStatusOk) return fail(PME_ETIMEOUT, "a grid barrier of the batch evaluation timed out");
+  return PME_OK;
+}
+
+int pme_batch_info(const pme_batch* b, int* nsys, int* grid, size_t* device_bytes) {
+  if (!b) return fail(PME_EINVAL, "batch is NULL");
+  if (nsys) *nsys = (int)b->desc.size();
+  if (grid) *grid = b->grid;
+  if (device_bytes) *device_bytes = b->bytes;
+  return PME_OK;
+}
+
+int pme_batch_set_stream(pme_batch* b, void* stream) {
+  if (!b) return fail(PME_EINVAL, "batch is NULL");
+  b->stream = (cudaStream_t)stream;
+  return PME_OK;
+}
+
+int pme_batch_set_trace(pme_batch* b, unsigned long long* dev_buf, int max_ctas) {
+  if (!b) return fail(PME_EINVAL, "batch is NULL");
+  if (dev_buf && max_ctas <= 0) return fail(PME_EINVAL, "max_ctas must be positive");
+  b->trace = dev_buf;
+  b->trace_ctas = dev_buf ? max_ctas : 0;
+  return PME_OK;
+}
+
+size_t pme_system_device_bytes(int nfftx, int nffty, int nfftz) {
+  return SystemState::bytes(nfftx, nffty, nfftz);
+}
 
 }  // extern "C"

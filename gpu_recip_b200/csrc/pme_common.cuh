@@ -22,20 +22,31 @@ struct Geom {
   int nx, ny, nz;       // grid
   int hx;               // nx/2 + 1 (half-complex extent along x)
   float rx, ry, rz;     // reciprocal box diagonal, FP32
+  float sx_hi, sy_hi, sz_hi;   // n_d * r_d as a float-float pair (hi + lo), used to map a
+  float sx_lo, sy_lo, sz_lo;   // coordinate to grid units without losing its low bits
 };
 
-// Fractional coordinate of one axis: fr = n * frac(x*r + 0.5) in [0, n); stencil origin i0 and
-// offset u in [0,1).  Follows CudaPMERecip.cu:510-529 (w = x r + 2, fr = n (w - (floor(w+0.5) -
-// 0.5))).  A non-finite or out-of-range fr maps to 0, so that no coordinate can index outside
-// the grid.
-__device__ __forceinline__ void frac_coord(float x, float r, int n, int& i0, float& u) {
-  float w = __fmaf_rn(x, r, 2.0f);
-  float t = __fsub_rn(floorf(__fadd_rn(w, 0.5f)), 0.5f);
-  float fr = __fmul_rn((float)n, __fsub_rn(w, t));
-  if (!(fr >= 0.0f && fr < (float)n)) fr = 0.0f;
-  int i = (int)fr;
+// Fractional coordinate of one axis in grid units: fr = n * frac(x*r + 1/2) in [0, n), split into
+// the stencil origin i0 and the offset u in [0, 1].  This is the function of
+// CudaPMERecip.cu:510-529 (fr = n (w - (floor(w + 0.5) - 0.5)), w = x r + 2), evaluated without
+// its FP32 cancellation: t = x (s_hi + s_lo) + n/2 is formed as p + e with p = fl(x s_hi) and
+// e = x s_lo + (x s_hi - p) exactly recovered with an FMA, so u carries ~1e-7 grid units of
+// error instead of ~1e-5.  Non-finite or huge inputs map to i0 = 0, u = 0.
+__device__ __forceinline__ void frac_coord(float x, float s_hi, float s_lo, int n, int& i0, float& u) {
+  float p = __fmul_rn(x, s_hi);
+  float e = __fmaf_rn(x, s_lo, __fmaf_rn(x, s_hi, -p));
+  if (!(fabsf(p) < 16777216.0f)) { p = 0.0f; e = 0.0f; }
+  const float fl = floorf(p);
+  float f = __fsub_rn(p, fl);
+  int i = (int)fl + (n >> 1);
+  if (n & 1) f = __fadd_rn(f, 0.5f);
+  float v = __fadd_rn(f, e);
+  if (v >= 1.0f) { v = __fsub_rn(v, 1.0f); i += 1; }
+  if (v < 0.0f) { v = __fadd_rn(v, 1.0f); i -= 1; }
+  i %= n;
+  if (i < 0) i += n;
   i0 = i;
-  u = __fsub_rn(fr, (float)i);
+  u = v;
 }
 
 // Cardinal B-spline weights of order P at offset u (weights of grid points i0..i0+P-1), built

@@ -17,16 +17,35 @@ namespace pme {
 constexpr int kMaxStages = 12;
 constexpr int kMaxFftLen = 512;
 
+// Division by a small constant d (1 <= d <= 2^16) as one multiply-high: x / d == umulhi(x, m)
+// with m = ceil(2^32 / d), exact for 0 <= x < 2^32 / d (all index ranges here are < 2^16).
+struct FastDiv {
+  unsigned int m;
+  int d;
+};
+
+__host__ __device__ inline FastDiv make_fastdiv(int d) {
+  FastDiv f;
+  f.d = d;
+  f.m = d <= 1 ? 0u : (unsigned int)((0x100000000ull + (unsigned long long)d - 1ull) / (unsigned long long)d);
+  return f;
+}
+
+__device__ __forceinline__ int fdiv(int x, const FastDiv& f) {
+  return f.d <= 1 ? x : (int)__umulhi((unsigned int)x, f.m);
+}
+
 struct FftPlan1D {
   int n;                    // transform length
   int nstages;
   int radix[kMaxStages];
+  FastDiv ns_div[kMaxStages];   // division by the stage's sub-transform length Ns
+  FastDiv n_div;                // division by n
   int tw_off;               // offset of this length's table in the twiddle array
 };
 
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
-  return make_float2(__fsub_rn(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y)),
-                     __fadd_rn(__fmul_rn(a.x, b.y), __fmul_rn(a.y, b.x)));
+  return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
 }
 __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
@@ -98,14 +117,15 @@ struct TileLane {
 // One Stockham stage over all lines of the tile.
 template <int R>
 __device__ __forceinline__ void fft_stage(const float2* __restrict__ in, float2* __restrict__ out,
-                                          int L, int Ns, int ld, const TileLane& ln,
-                                          const float2* tw, bool inv) {
+                                          int L, int Ns, const FastDiv& nsd, int ld,
+                                          const TileLane& ln, const float2* tw, bool inv) {
   const int nb = L / R;
   const int tstride = L / (Ns * R);
   const int t = ln.t;
   if (!ln.active()) return;
   for (int j = ln.y; j < nb; j += ln.ny) {
-    const int k = j % Ns;
+    const int blk = fdiv(j, nsd);
+    const int k = j - blk * Ns;
     float2 v[R];
 #pragma unroll
     for (int r = 0; r < R; r++) v[r] = in[(j + r * nb) * ld + t];
@@ -116,7 +136,7 @@ __device__ __forceinline__ void fft_stage(const float2* __restrict__ in, float2*
       v[r] = cmul(v[r], w);
     }
     dft_small<R>(v, inv);
-    const int base = (j / Ns) * Ns * R + k;
+    const int base = blk * Ns * R + k;
 #pragma unroll
     for (int u = 0; u < R; u++) out[(base + u * Ns) * ld + t] = v[u];
   }
@@ -134,11 +154,12 @@ __device__ __forceinline__ float2* fft_tile(float2* buf0, float2* buf1, const Ff
   const int L = plan.n;
   for (int s = 0; s < plan.nstages; s++) {
     const int R = plan.radix[s];
+    const FastDiv nsd = plan.ns_div[s];
     switch (R) {
-      case 4: fft_stage<4>(src, dst, L, Ns, ld, ln, tw, inv); break;
-      case 2: fft_stage<2>(src, dst, L, Ns, ld, ln, tw, inv); break;
-      case 3: fft_stage<3>(src, dst, L, Ns, ld, ln, tw, inv); break;
-      case 5: fft_stage<5>(src, dst, L, Ns, ld, ln, tw, inv); break;
+      case 4: fft_stage<4>(src, dst, L, Ns, nsd, ld, ln, tw, inv); break;
+      case 2: fft_stage<2>(src, dst, L, Ns, nsd, ld, ln, tw, inv); break;
+      case 3: fft_stage<3>(src, dst, L, Ns, nsd, ld, ln, tw, inv); break;
+      case 5: fft_stage<5>(src, dst, L, Ns, nsd, ld, ln, tw, inv); break;
       default: break;
     }
     __syncthreads();

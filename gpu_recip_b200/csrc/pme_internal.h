@@ -6,66 +6,46 @@
 
 #include "pme_common.cuh"
 #include "pme_fft.cuh"
+#include "pme_tiles.cuh"
 
 namespace pme {
 
-// Energy/virial record layout in device memory (doubles).  Accumulated, never overwritten,
-// like the reference's CudaEnergyVirial slots (CudaEnergyVirial.cu:158-167).
-enum EvSlot { kEvRecip = 0, kEvSelf = 1, kEvVirial = 2, kEvCount = 11 };
+constexpr int kPhases = 7;
 
-// Per-axis line-FFT tiling of one pass.
-struct PassTiling {
-  int tx;        // lines per CTA tile
-  int ny;        // threadIdx.y extent (butterfly lanes)
+// Device status word values (fused kernel).
+enum { kStatusOk = 0, kStatusBarrierTimeout = 1 };
+
+// Arguments of the persistent fused kernel.  A single system travels by value (`single`, with
+// table == nullptr); a batch uses a device table of descriptors and per-phase tile prefix sums
+// prefix[ph * (nsys + 1) + s].
+struct FusedArgs {
+  const SysDesc* table;
+  SysDesc single;
+  int nsys;
+  const int* prefix;
+  int total[kPhases];
+  unsigned int* bar;         // [arrival count, generation], zero-initialised
+  int* status;               // kStatus*; sticky until cleared by the host
+  unsigned int spin_limit;   // barrier polls before giving up
+  int inject;                // 1: CTA 0 leaves before the first barrier (failure-detection test)
+  unsigned long long* trace; // optional: [cta][phase][begin, end] %globaltimer stamps
+  int trace_ctas;            // CTAs recorded (rows of trace)
 };
 
-// Deterministic cross-CTA reduction scratch: per-CTA partials and a ticket counter that the
-// last CTA resets.
-struct ReduceScratch {
-  double* partials;      // [max_blocks][8]
-  unsigned int* ticket;  // one counter per reduction site
-  int max_blocks;
-};
+cudaError_t configure_kernels(size_t* max_dyn_smem);
 
-// Solve parameters (CudaPMERecip.cu:1988-2012: fac = pi^2/kappa^2, piv_inv = 1/(pi V)).
-struct SolveParams {
-  float fac;
-  float piv_inv;
-  const float* bmx;   // B-spline moduli, FP32 (1/|b|^2)
-  const float* bmy;
-  const float* bmz;
-  int calc_ev;
-  double* ev;         // energy/virial record
-};
+size_t spread_smem(int order);
+size_t fused_smem_bytes(const SysDesc& d);
+void fused_tile_counts(const SysDesc& d, int* counts);
 
-enum ForceKind { kForceF32Soa = 0, kForceF32x3 = 1, kForceI64SoaAccum = 2 };
+cudaError_t staged_spread(const SysDesc& d, cudaStream_t s);
+cudaError_t staged_self(const SysDesc& d, cudaStream_t s);
+cudaError_t staged_r2c(const SysDesc& d, bool zero_accum, cudaStream_t s);
+cudaError_t staged_solve(const SysDesc& d, cudaStream_t s);
+cudaError_t staged_c2r(const SysDesc& d, cudaStream_t s);
+cudaError_t staged_gather(const SysDesc& d, cudaStream_t s);
 
-cudaError_t launch_spread(const float4* xyzq, int n, const Geom& g, int order,
-                          unsigned long long* accum, cudaStream_t s);
-
-cudaError_t launch_x_r2c(const long long* accum, float2* cgrid, const Geom& g,
-                         const FftPlan1D& px, const float2* tw, const PassTiling& t,
-                         cudaStream_t s);
-
-// Complex passes along y (axis 1) or z (axis 2) of the half-complex grid [z][y][kx].
-// mode: 0 forward, 1 inverse, 2 forward + solve + inverse (axis 2 only), 3 solve only (axis 2).
-cudaError_t launch_c2c(float2* cgrid, const Geom& g, int axis, int mode, const FftPlan1D& plan,
-                       const float2* tw, const PassTiling& t, const SolveParams* sp,
-                       const ReduceScratch& rs, int rs_site, cudaStream_t s);
-
-cudaError_t launch_x_c2r(const float2* cgrid, float* rgrid, const Geom& g, const FftPlan1D& px,
-                         const float2* tw, const PassTiling& t, cudaStream_t s);
-
-cudaError_t launch_gather(const float4* xyzq, int n, const Geom& g, int order, const float* rgrid,
-                          int kind, int stride, void* force, cudaStream_t s);
-
-cudaError_t launch_self_energy(const float4* xyzq, int n, double kappa, double* ev,
-                               const ReduceScratch& rs, int rs_site, cudaStream_t s);
-
-cudaError_t launch_fixed_to_float(const long long* accum, float* out, size_t count,
-                                  cudaStream_t s);
-
-size_t c2c_smem_bytes(int L, const PassTiling& t);
-int c2c_num_blocks(const Geom& g, int axis, const PassTiling& t);
+cudaError_t fused_launch(const FusedArgs& a, int grid, size_t smem, cudaStream_t s);
+cudaError_t fused_max_grid(size_t smem, int* grid);
 
 }  // namespace pme

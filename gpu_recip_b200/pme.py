@@ -242,6 +242,28 @@ class CudaPMERecip:
         C.check(self._lib.pme_load_charge_grid(self._h, g.ctypes.data_as(ctypes.c_void_p)),
                 "load_charge_grid")
 
+    # -- failure detection ----------------------------------------------------------------------
+    def get_status(self) -> int:
+        """Synchronise; raise PMEError(PME_ETIMEOUT) if a fused evaluation's barrier wait gave up
+        (the sticky device status is cleared and the handle reset), else return 0."""
+        st = ctypes.c_int()
+        C.check(self._lib.pme_get_status(self._h, ctypes.byref(st)), "get_status")
+        return st.value
+
+    def set_barrier_spin_limit(self, polls: int):
+        C.check(self._lib.pme_set_barrier_spin_limit(self._h, int(polls)), "set_barrier_spin_limit")
+
+    def set_trace(self, buf, max_ctas: int = 0):
+        """Record per-CTA, per-phase %globaltimer stamps of fused evaluations into ``buf`` (int64
+        device tensor of max_ctas*14 entries); None turns it off."""
+        if buf is None:
+            C.check(self._lib.pme_set_trace(self._h, None, 0), "set_trace")
+        else:
+            C.check(self._lib.pme_set_trace(self._h, _ptr(buf), int(max_ctas or buf.numel() // 14)), "set_trace")
+
+    def set_fault_injection(self, what: int):
+        C.check(self._lib.pme_set_fault_injection(self._h, int(what)), "set_fault_injection")
+
     def solved_grid(self) -> np.ndarray:
         nx, ny, nz = self.nfft
         out = np.empty((nz, ny, nx), dtype=np.float32)
@@ -270,3 +292,96 @@ class CudaDomdecRecip:
             stride = 1 if (force.dim() == 2 and force.shape[1] == 3) else force.numel() // 3
         self.pme.eval_ortho((inv_boxx, inv_boxy, inv_boxz), coord, ncoord, self.kappa, calc_energy,
                             calc_virial, force, stride)
+
+
+class PmeBatch:
+    """Many independent systems evaluated by one persistent launch (pme_batch_* of the C ABI).
+
+    ``systems`` is a sequence of dicts with keys nfft (3,), order, box (3,), kappa, xyzq (device
+    float32 (N,4) tensor), force (device tensor) and optionally force_kind, stride, calc_energy,
+    calc_virial.  Device tensors must stay alive while the batch is used."""
+
+    def __init__(self, systems, stream=None):
+        lib = C.load()
+        n = len(systems)
+        arr = (C.SystemDesc * n)()
+        self._keep = []
+        for i, s in enumerate(systems):
+            x, f = s["xyzq"], s["force"]
+            natom = int(s.get("natom", x.shape[0]))
+            kind = s.get("force_kind")
+            stride = int(s.get("stride", 0))
+            if kind is None:
+                kind = CudaPMERecip._force_kind(f, stride)
+            nx, ny, nz = s["nfft"]
+            arr[i].nfftx, arr[i].nffty, arr[i].nfftz = int(nx), int(ny), int(nz)
+            arr[i].order = int(s["order"])
+            arr[i].natom = natom
+            for d in range(3):
+                arr[i].box[d] = float(s["box"][d])
+            arr[i].kappa = float(s["kappa"])
+            arr[i].xyzq = _xyzq_ptr(x, natom).value
+            arr[i].force = _ptr(f).value
+            arr[i].force_kind = int(kind)
+            arr[i].stride = stride
+            arr[i].calc_energy = int(s.get("calc_energy", True))
+            arr[i].calc_virial = int(s.get("calc_virial", True))
+            self._keep.append((x, f))
+        h = ctypes.c_void_p()
+        C.check(lib.pme_batch_create(ctypes.cast(arr, ctypes.c_void_p), n,
+                                     ctypes.c_void_p(_stream_handle(stream)), ctypes.byref(h)),
+                "pme_batch_create")
+        self._h = h
+        self._lib = lib
+        self.nsys = n
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self._lib.pme_batch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream):
+        C.check(self._lib.pme_batch_set_stream(self._h, ctypes.c_void_p(_stream_handle(stream))), "set_stream")
+
+    def set_system(self, i: int, box=None, xyzq=None, force=None):
+        b = (ctypes.c_double * 3)(*[float(v) for v in box]) if box is not None else None
+        C.check(self._lib.pme_batch_set_system(self._h, int(i), b, _ptr(xyzq) if xyzq is not None else None,
+                                               _ptr(force) if force is not None else None), "set_system")
+
+    def commit(self):
+        C.check(self._lib.pme_batch_commit(self._h), "commit")
+
+    def eval(self):
+        C.check(self._lib.pme_batch_eval(self._h), "batch eval")
+
+    def clear_energy_virial(self):
+        C.check(self._lib.pme_batch_clear_energy_virial(self._h), "batch clear")
+
+    def energy_virial(self) -> np.ndarray:
+        """(nsys, 11): [E_recip, E_self, W_xx .. W_zz] per system (synchronising)."""
+        out = np.zeros((self.nsys, C.PME_EV_COUNT))
+        C.check(self._lib.pme_batch_get_energy_virial(self._h, out.ctypes.data_as(C._DP)), "batch ev")
+        return out
+
+    def set_trace(self, buf, max_ctas: int = 0):
+        if buf is None:
+            C.check(self._lib.pme_batch_set_trace(self._h, None, 0), "set_trace")
+        else:
+            C.check(self._lib.pme_batch_set_trace(self._h, _ptr(buf), int(max_ctas or buf.numel() // 14)), "set_trace")
+
+    def info(self):
+        n = ctypes.c_int()
+        g = ctypes.c_int()
+        b = ctypes.c_size_t()
+        C.check(self._lib.pme_batch_info(self._h, ctypes.byref(n), ctypes.byref(g), ctypes.byref(b)), "info")
+        return {"nsys": n.value, "grid_ctas": g.value, "device_bytes": b.value}
+
+
+def system_device_bytes(nfft) -> int:
+    return int(C.load().pme_system_device_bytes(int(nfft[0]), int(nfft[1]), int(nfft[2])))

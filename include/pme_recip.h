@@ -16,6 +16,8 @@
 #ifndef PME_RECIP_H
 #define PME_RECIP_H
 
+#include <stddef.h>
+
 #if defined(__GNUC__)
 #define PME_API __attribute__((visibility("default")))
 #else
@@ -108,6 +110,60 @@ PME_API int pme_copy_solved_grid(pme_recip* h, float* host_out);             /* 
 /* Replace the accumulated charge grid (e.g. to test the transforms on a known grid): host
  * float nx*ny*nz values rounded to the 2^40 fixed point; synchronous. */
 PME_API int pme_load_charge_grid(pme_recip* h, const float* host_in);
+
+/* ---- device status of the fused evaluation ----
+ * The fused evaluation (pme_eval_ortho) runs as one cooperative kernel whose grid barriers wait
+ * at most a bounded number of polls.  If a wait gives up, the kernel stops early, leaves a sticky
+ * status on the device and later evaluations do nothing until it is cleared.  pme_get_status
+ * synchronises the stream, reports the status (PME_ETIMEOUT if a wait gave up) and clears it,
+ * together with the barrier words and the accumulation grid, so the handle is usable again. */
+PME_API int pme_get_status(pme_recip* h, int* device_status);
+PME_API int pme_set_barrier_spin_limit(pme_recip* h, unsigned int polls);   /* default 2^22 */
+/* Test hook for failure detection: PME_INJECT_SKIP_BARRIER makes CTA 0 of the next fused
+ * evaluations leave before the first grid barrier, so the other CTAs' bounded waits run out
+ * (no fault, no hang).  PME_INJECT_NONE turns it off. */
+enum { PME_INJECT_NONE = 0, PME_INJECT_SKIP_BARRIER = 1 };
+PME_API int pme_set_fault_injection(pme_recip* h, int what);
+
+/* Profiling hook: while set, every fused evaluation writes, for each CTA c < max_ctas and each of
+ * its 7 phases p (spread, x fwd, y fwd, z fwd+solve+inv, y inv, x inv, gather), the %globaltimer
+ * (ns) at the phase's start and end to dev_buf[(c * 7 + p) * 2 + {0, 1}] (device memory,
+ * max_ctas * 14 entries).  NULL turns it off. */
+PME_API int pme_set_trace(pme_recip* h, unsigned long long* dev_buf, int max_ctas);
+
+/* ---- batches: many independent systems in one persistent launch ----
+ * Each system has its own grid, spline order, box, kappa, coordinates and force output; all
+ * device state (grids, plans, moduli, records) is allocated once at creation, so repeated
+ * evaluations allocate nothing.  This path has no counterpart in the reference (which evaluates
+ * one system per CudaPMERecip instance). */
+typedef struct pme_batch pme_batch;
+typedef struct {
+  int nfftx, nffty, nfftz, order;
+  int natom;
+  double box[3];          /* orthorhombic box edges (A) */
+  double kappa;
+  const void* xyzq;       /* device float4[natom] */
+  void* force;            /* device output of force_kind */
+  int force_kind;
+  int stride;             /* SoA stride (>= natom) for PME_FORCE_F32_SOA / I64 kinds */
+  int calc_energy, calc_virial;
+} pme_system_desc;
+
+PME_API int pme_batch_create(const pme_system_desc* systems, int nsys, void* stream, pme_batch** out);
+PME_API int pme_batch_destroy(pme_batch* b);
+PME_API int pme_batch_set_stream(pme_batch* b, void* stream);
+/* Change one system's box (NULL keeps it), coordinates or force pointer (NULL keeps them);
+ * takes effect at the next pme_batch_commit. */
+PME_API int pme_batch_set_system(pme_batch* b, int sys, const double* box3, const void* xyzq, void* force);
+PME_API int pme_batch_commit(pme_batch* b);      /* uploads descriptors (synchronises the stream) */
+PME_API int pme_batch_eval(pme_batch* b);        /* one launch: every system, every stage */
+PME_API int pme_batch_clear_energy_virial(pme_batch* b);
+/* Synchronises; out = nsys * PME_EV_COUNT doubles, system-major. */
+PME_API int pme_batch_get_energy_virial(pme_batch* b, double* out);
+PME_API int pme_batch_info(const pme_batch* b, int* nsys, int* grid_ctas, size_t* device_bytes);
+PME_API int pme_batch_set_trace(pme_batch* b, unsigned long long* dev_buf, int max_ctas);
+/* Device bytes one system of this grid occupies (for admission by HBM footprint). */
+PME_API size_t pme_system_device_bytes(int nfftx, int nffty, int nfftz);
 
 /* ---- errors / version ---- */
 PME_API const char* pme_last_error_string(void);     /* thread-local message of the last failure */

@@ -108,7 +108,7 @@ def spread_f64(xyzq, recip3, nfft, order, nthreads=0) -> np.ndarray:
 def spread_fixed(xyzq, recip3, nfft, order, nthreads=0) -> np.ndarray:
     """int64 fixed-point grid (scale 2^40) from the FP32 mirror of the GPU spreading."""
     x = np.ascontiguousarray(xyzq, dtype=np.float32).reshape(-1, 4)
-    r = np.ascontiguousarray(np.asarray(recip3, dtype=np.float64).astype(np.float32))
+    r = np.ascontiguousarray(recip3, dtype=np.float64)
     nx, ny, nz = nfft
     g = np.zeros((nz, ny, nx), dtype=np.int64)
     _check(lib().orc_spread_fixed(_p(x), x.shape[0], _p(r), nx, ny, nz, order, _p(g), nthreads),

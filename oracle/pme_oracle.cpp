@@ -106,17 +106,31 @@ static void bspline_f32(int p, float u, float* th) {
   }
 }
 
-// Fractional coordinate and stencil origin, FP32 mirror of the kernel (CudaPMERecip.cu:510-529).
-// fr = n * frac(x*r + 0.5) in [0, n); a non-finite or out-of-range fr is mapped to 0 (the kernel
-// does the same so that no input can index outside the grid).
-static inline void frac_f32(float x, float r, int n, int* i0, float* u) {
-  float w = std::fmaf(x, r, 2.0f);
-  float t = std::floor(w + 0.5f) - 0.5f;
-  float fr = (float)n * (w - t);
-  if (!(fr >= 0.0f && fr < (float)n)) fr = 0.0f;
-  int i = (int)fr;
+// Fractional coordinate in grid units, FP32 mirror of the kernel: fr = n * frac(x*r + 1/2)
+// (the function of CudaPMERecip.cu:510-529), evaluated as p + e with p = fl(x s_hi) and the
+// product's rounding error recovered by fmaf, s_hi + s_lo = n r as a float-float pair.
+// Non-finite or huge inputs map to i0 = 0, u = 0.
+static inline void frac_f32(float x, float s_hi, float s_lo, int n, int* i0, float* u) {
+  float p = x * s_hi;
+  float e = std::fmaf(x, s_lo, std::fmaf(x, s_hi, -p));
+  if (!(std::fabs(p) < 16777216.0f)) { p = 0.0f; e = 0.0f; }
+  const float fl = std::floor(p);
+  float f = p - fl;
+  int i = (int)fl + (n >> 1);
+  if (n & 1) f = f + 0.5f;
+  float v = f + e;
+  if (v >= 1.0f) { v = v - 1.0f; i += 1; }
+  if (v < 0.0f) { v = v + 1.0f; i -= 1; }
+  i %= n;
+  if (i < 0) i += n;
   *i0 = i;
-  *u = fr - (float)i;
+  *u = v;
+}
+
+static inline void split_scale(double r, int n, float* hi, float* lo) {
+  const double s = r * (double)n;
+  *hi = (float)s;
+  *lo = (float)(s - (double)*hi);
 }
 
 static inline void frac_f64(double x, double r, int n, int* i0, double* u) {
@@ -175,15 +189,19 @@ extern "C" int orc_spread_f64(const double* xyzq, int natom, const double* recip
 
 // Fixed-point spreading, FP32 mirror: each contribution is ((q*thx[a])*thy[b])*thz[c] in FP32,
 // scaled by 2^40 and rounded to nearest-even int64 (CudaPMERecip.cu:44-66 write_grid<long long>).
-extern "C" int orc_spread_fixed(const float* xyzq, int natom, const float* recip3f,
+extern "C" int orc_spread_fixed(const float* xyzq, int natom, const double* recip3,
                                 int nx, int ny, int nz, int p, int64_t* grid, int nthreads) {
   if (natom < 0 || nx < p || ny < p || nz < p || p < 2 || p > 16) return -1;
   const size_t G = (size_t)nx * ny * nz;
   std::fill(grid, grid + G, (int64_t)0);
+  float shi[3], slo[3];
+  split_scale(recip3[0], nx, &shi[0], &slo[0]);
+  split_scale(recip3[1], ny, &shi[1], &slo[1]);
+  split_scale(recip3[2], nz, &shi[2], &slo[2]);
   std::vector<int> iz0(natom);
   for (int i = 0; i < natom; i++) {
     float u;
-    frac_f32(xyzq[4 * i + 2], recip3f[2], nz, &iz0[i], &u);
+    frac_f32(xyzq[4 * i + 2], shi[2], slo[2], nz, &iz0[i], &u);
   }
   parallel_for(hw_threads(nthreads), nz, [&](int z) {
     float thx[16], thy[16], thz[16];
@@ -193,9 +211,9 @@ extern "C" int orc_spread_fixed(const float* xyzq, int natom, const float* recip
       if (c >= p) continue;
       int ix, iy, izz;
       float ux, uy, uz;
-      frac_f32(xyzq[4 * i + 0], recip3f[0], nx, &ix, &ux);
-      frac_f32(xyzq[4 * i + 1], recip3f[1], ny, &iy, &uy);
-      frac_f32(xyzq[4 * i + 2], recip3f[2], nz, &izz, &uz);
+      frac_f32(xyzq[4 * i + 0], shi[0], slo[0], nx, &ix, &ux);
+      frac_f32(xyzq[4 * i + 1], shi[1], slo[1], ny, &iy, &uy);
+      frac_f32(xyzq[4 * i + 2], shi[2], slo[2], nz, &izz, &uz);
       bspline_f32(p, ux, thx);
       bspline_f32(p, uy, thy);
       bspline_f32(p, uz, thz);
