@@ -55,7 +55,9 @@ SIGNATURES = {
     "pme_load_charge_grid": [_P, _P],
     "pme_get_status": [_P, ctypes.POINTER(_I)],
     "pme_set_barrier_spin_limit": [_P, ctypes.c_uint],
+    "pme_reserve_atoms": [_P, _I],
     "pme_set_fault_injection": [_P, _I],
+    "pme_set_fft_schedule": [_P, _I],
     "pme_batch_create": [_P, _I, _P, ctypes.POINTER(_P)],
     "pme_batch_destroy": [_P],
     "pme_batch_set_stream": [_P, _P],
@@ -76,6 +78,7 @@ _RESTYPES = {"pme_last_error_string": ctypes.c_char_p, "pme_status_string": ctyp
              "pme_system_device_bytes": ctypes.c_size_t}
 
 PME_INJECT_NONE, PME_INJECT_SKIP_BARRIER = 0, 1
+PME_SCHED_AUTO, PME_SCHED_PLANES, PME_SCHED_PASSES = 0, 1, 2
 
 
 class SystemDesc(ctypes.Structure):

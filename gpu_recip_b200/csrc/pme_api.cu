@@ -165,7 +165,10 @@ size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 struct SystemState {
   int nx = 0, ny = 0, nz = 0, order = 0;
   FftPlan1D px{}, py{}, pz{};
-  int tx_rows = 0, tx_y = 0, tx_z = 0;
+  int tx_rows = 0, tx_y = 0, tx_z = 0, plane = 0;
+  int bry = 4, brz = 4, nby = 1, nbz = 1;
+  int bin_cap = 0, atom_cap = 0;
+  int* bins = nullptr;       // [2 nbins counts][nbins*bin_cap atoms][2 ovf counts][atom_cap ovf]
   unsigned long long* accum = nullptr;
   float2* cgrid = nullptr;
   float* rgrid = nullptr;
@@ -194,8 +197,25 @@ struct SystemState {
     py.tw_off = nx;
     pz.tw_off = nx + ny;
     tx_rows = pick_rows_tile(nx);
-    tx_y = pick_cols_tile(nx / 2 + 1, ny);
-    tx_z = pick_cols_tile(nx / 2 + 1, nz);
+    tx_y = pick_rows_tile(ny);
+    tx_z = pick_cols_tile(ny, nz);
+    // whole-plane tiles need one thread per line of each orientation and the plane in smem
+    plane = (plane_smem_bytes(ny, nz) <= kTileSmemBudget && ny <= kThreads && nz <= kThreads) ? 1 : 0;
+    // row blocks of the fused spread + x pass: the largest square block that fits
+    for (int b = 4; b >= 1; b--) {
+      bry = brz = b;
+      if (spread_x_smem_bytes(nx, b * b) <= kTileSmemBudget) break;
+    }
+    nby = (ny + bry - 1) / bry;
+    nbz = (nz + brz - 1) / brz;
+  }
+
+  int nbins() const { return nby * nbz; }
+
+  // bin storage for up to natom atoms: capacity 1.5x the mean occupancy + 32 per bin
+  static int cap_for(int natom, int nbins) { return std::max(32, (int)(1.5 * natom / nbins) + 32); }
+  size_t bin_ints(int natom) const {
+    return 2 * (size_t)nbins() + (size_t)nbins() * cap_for(natom, nbins()) + 2 + (size_t)std::max(natom, 1);
   }
 
   void carve(char* base) {
@@ -260,6 +280,8 @@ struct SystemState {
     d.rxd = r[0]; d.ryd = r[1]; d.rzd = r[2];
     d.fac = kappa > 0.0 ? kPi * kPi / (kappa * kappa) : 0.0;
     d.piv_inv = r[0] * r[1] * r[2] / kPi;
+    d.fac_f = (float)d.fac;
+    d.piv_inv_f = (float)d.piv_inv;
     d.calc_ev = calc_ev;
     d.calc_self = calc_self;
     d.self_coef = -kappa * kCcelec / std::sqrt(kPi);
@@ -276,6 +298,16 @@ struct SystemState {
     d.acc = acc;
     d.ev = ev;
     d.tx_rows = tx_rows; d.tx_y = tx_y; d.tx_z = tx_z;
+    d.plane = plane;
+    d.bry = bry; d.brz = brz; d.nby = nby; d.nbz = nbz;
+    d.bin_cap = bin_cap;
+    if (bins) {
+      const size_t nb = nbins();
+      d.bin_count = bins;
+      d.bin_atoms = bins + 2 * nb;
+      d.ovf_count = bins + 2 * nb + nb * (size_t)bin_cap;
+      d.ovf_atoms = d.ovf_count + 2;
+    }
     return d;
   }
 };
@@ -284,11 +316,12 @@ struct SystemState {
 
 struct pme_recip {
   int fft_type = PME_FFT_BOX;
+  int* d_bins = nullptr;
   int device = 0;
   cudaStream_t stream = nullptr;
   SystemState st;
   char* d_block = nullptr;
-  unsigned int* d_bar = nullptr;
+  unsigned long long* d_bar = nullptr;
   int* d_status = nullptr;
   bool accum_dirty = false;
   size_t max_smem = 0;
@@ -296,6 +329,7 @@ struct pme_recip {
   int inject = 0;
   unsigned long long* trace = nullptr;
   int trace_ctas = 0;
+  int plane_mode = 0;   // 0 automatic, 1 whole-plane tiles where they fit, 2 separate passes
 };
 
 struct pme_batch {
@@ -307,7 +341,7 @@ struct pme_batch {
   int* d_prefix = nullptr;
   int total[kPhases] = {0};
   char* d_block = nullptr;
-  unsigned int* d_bar = nullptr;
+  unsigned long long* d_bar = nullptr;
   int* d_status = nullptr;
   size_t smem = 0;
   int grid = 0;
@@ -321,12 +355,37 @@ namespace {
 
 void release(pme_recip* h) {
   if (!h) return;
+  cudaFree(h->d_bins);
   cudaFree(h->d_block);
   cudaFree(h->d_bar);
   delete h;
 }
 
 int handle_ok(const pme_recip* h) { return h ? PME_OK : fail(PME_EINVAL, "handle is NULL"); }
+
+// Size the fused path's atom bins for natom atoms (allocates only when the count grows).
+int ensure_bins(pme_recip* h, int natom) {
+  SystemState& s = h->st;
+  if (h->d_bins && natom <= s.atom_cap) return PME_OK;
+  const int cap = std::max(natom, 1024);
+  const size_t ints = s.bin_ints(cap);
+  cudaError_t e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "bins: sync");
+  cudaFree(h->d_bins);
+  h->d_bins = nullptr;
+  if (cudaMalloc(&h->d_bins, ints * sizeof(int)) != cudaSuccess) {
+    cudaGetLastError();
+    s.bins = nullptr;
+    s.atom_cap = 0;
+    return fail(PME_ENOMEM, "device allocation of the atom bins failed");
+  }
+  e = cudaMemset(h->d_bins, 0, ints * sizeof(int));
+  if (e != cudaSuccess) return cuda_fail(e, "bins: clear");
+  s.bins = h->d_bins;
+  s.atom_cap = cap;
+  s.bin_cap = SystemState::cap_for(cap, s.nbins());
+  return PME_OK;
+}
 
 // 3 doubles of the reciprocal diagonal
 void diag3(const double* recip, double* r3) {
@@ -335,20 +394,29 @@ void diag3(const double* recip, double* r3) {
   r3[2] = recip[8];
 }
 
-int launch_fused_single(pme_recip* h, const SysDesc& d) {
+int launch_fused_single(pme_recip* h, const SysDesc& d_in) {
+  SysDesc d = d_in;
   FusedArgs a;
   std::memset(&a, 0, sizeof(a));
   a.table = nullptr;
-  a.single = d;
   a.nsys = 1;
   a.prefix = nullptr;
-  fused_tile_counts(d, a.total);
   a.bar = h->d_bar;
   a.status = h->d_status;
   a.spin_limit = h->spin_limit;
   a.inject = h->inject;
   a.trace = h->trace;
   a.trace_ctas = h->trace_ctas;
+  if (h->trace) d.steps = h->trace + (size_t)h->trace_ctas * kPhases * 2;
+  // whole-plane tiles only pay when there are enough planes to occupy the GPU; otherwise the
+  // separate y and z passes spread the same work over many more CTAs
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
+  if (h->plane_mode == 0) d.plane = (d.plane && d.g.hx >= sms) ? 1 : 0;
+  else d.plane = (d.plane && h->plane_mode == 1) ? 1 : 0;
+  fused_tile_counts(d, a.total);
+  a.nbar = fused_barriers(a.total);
+  a.single = d;
   const size_t smem = fused_smem_bytes(d);
   int grid = 0;
   cudaError_t e = fused_max_grid(smem, &grid);
@@ -387,7 +455,7 @@ int pme_create(int nfftx, int nffty, int nfftz, int order, int fft_type, int nno
   h->st.setup(nfftx, nffty, nfftz, order);
   const size_t bytes = SystemState::bytes(nfftx, nffty, nfftz);
   if (cudaMalloc(&h->d_block, bytes) != cudaSuccess ||
-      cudaMalloc(&h->d_bar, 4 * sizeof(unsigned int)) != cudaSuccess) {
+      cudaMalloc(&h->d_bar, 4 * sizeof(unsigned long long)) != cudaSuccess) {
     cudaGetLastError();
     release(h);
     return fail(PME_ENOMEM, "device allocation failed");
@@ -395,7 +463,7 @@ int pme_create(int nfftx, int nffty, int nfftz, int order, int fft_type, int nno
   h->d_status = (int*)(h->d_bar + 2);
   h->st.carve(h->d_block);
   e = cudaMemset(h->d_block, 0, bytes);
-  if (e == cudaSuccess) e = cudaMemset(h->d_bar, 0, 4 * sizeof(unsigned int));
+  if (e == cudaSuccess) e = cudaMemset(h->d_bar, 0, 4 * sizeof(unsigned long long));
   if (e == cudaSuccess) e = h->st.upload_tables();
   if (e != cudaSuccess) {
     release(h);
@@ -583,6 +651,7 @@ int pme_eval_ortho(pme_recip* h, double inv_boxx, double inv_boxy, double inv_bo
     if (e != cudaSuccess) return cuda_fail(e, "eval: clear grid");
     h->accum_dirty = false;
   }
+  if (int rc = ensure_bins(h, ncoord)) return rc;
   const double r3[3] = {inv_boxx, inv_boxy, inv_boxz};
   const int ev = (calc_energy || calc_virial) ? 1 : 0;
   SysDesc d = h->st.desc(r3, kappa, xyzq, ncoord, force, kind, stride, ev, calc_energy ? 1 : 0);
@@ -613,8 +682,18 @@ int pme_copy_charge_grid(pme_recip* h, float* host_out) {
 }
 
 int pme_copy_fft_grid(pme_recip* h, float* host_out) {
-  if (int rc = handle_ok(h)) return rc;
-  return copy_back(h, host_out, h->st.cgrid, h->st.H() * 8, "copy_fft_grid");
+  if (!h || !host_out) return fail(PME_EINVAL, "NULL argument");
+  const SystemState& s = h->st;
+  std::vector<float2> tmp(s.H());
+  int rc = copy_back(h, tmp.data(), s.cgrid, s.H() * 8, "copy_fft_grid");
+  if (rc) return rc;
+  const int hx = s.nx / 2 + 1;
+  float2* out = (float2*)host_out;
+  for (int kx = 0; kx < hx; kx++)
+    for (int z = 0; z < s.nz; z++)
+      for (int y = 0; y < s.ny; y++)
+        out[((size_t)z * s.ny + y) * hx + kx] = tmp[((size_t)kx * s.nz + z) * s.ny + y];
+  return PME_OK;
 }
 
 int pme_copy_solved_grid(pme_recip* h, float* host_out) {
@@ -649,9 +728,11 @@ int pme_get_status(pme_recip* h, int* device_status) {
   if (status != kStatusOk) {
     // clear the sticky status, the barrier words, the accumulation grid and the accumulators
     // (an interrupted evaluation leaves them partly filled) so the handle is usable again
-    e = cudaMemsetAsync(h->d_bar, 0, 4 * sizeof(unsigned int), h->stream);
+    e = cudaMemsetAsync(h->d_bar, 0, 4 * sizeof(unsigned long long), h->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(h->st.accum, 0, h->st.G() * 8, h->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(h->st.acc, 0, kAccCount * sizeof(long long), h->stream);
+    if (e == cudaSuccess && h->d_bins)
+      e = cudaMemsetAsync(h->d_bins, 0, h->st.bin_ints(h->st.atom_cap) * sizeof(int), h->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) return cuda_fail(e, "get_status: reset");
     return fail(PME_ETIMEOUT, "a grid barrier of the fused evaluation timed out");
@@ -659,9 +740,23 @@ int pme_get_status(pme_recip* h, int* device_status) {
   return PME_OK;
 }
 
+int pme_reserve_atoms(pme_recip* h, int natom) {
+  if (int rc = handle_ok(h)) return rc;
+  if (natom < 0) return fail(PME_EINVAL, "natom must be >= 0");
+  DeviceGuard dg(h->device);
+  return ensure_bins(h, natom);
+}
+
 int pme_set_barrier_spin_limit(pme_recip* h, unsigned int polls) {
   if (int rc = handle_ok(h)) return rc;
   h->spin_limit = polls == 0 ? 1u : polls;
+  return PME_OK;
+}
+
+int pme_set_fft_schedule(pme_recip* h, int schedule) {
+  if (int rc = handle_ok(h)) return rc;
+  if (schedule < PME_SCHED_AUTO || schedule > PME_SCHED_PASSES) return fail(PME_EINVAL, "unknown schedule");
+  h->plane_mode = schedule;
   return PME_OK;
 }
 
@@ -732,17 +827,21 @@ int pme_batch_create(const pme_system_desc* systems, int nsys, void* stream, pme
   if (e == cudaSuccess) e = configure_kernels(&max_smem);
   if (e != cudaSuccess) { delete b; return cuda_fail(e, "batch: configure kernels"); }
   b->st.resize(nsys);
-  std::vector<size_t> off(nsys);
+  std::vector<size_t> off(nsys), boff(nsys);
   size_t total = 0;
   for (int i = 0; i < nsys; i++) {
     b->st[i].setup(systems[i].nfftx, systems[i].nffty, systems[i].nfftz, systems[i].order);
     off[i] = total;
     total += SystemState::bytes(systems[i].nfftx, systems[i].nffty, systems[i].nfftz);
   }
+  for (int i = 0; i < nsys; i++) {
+    boff[i] = total;
+    total += align256(b->st[i].bin_ints(systems[i].natom) * sizeof(int));
+  }
   b->bytes = total;
   const size_t table_bytes = align256(sizeof(SysDesc) * nsys) + align256(sizeof(int) * kPhases * (nsys + 1));
   if (cudaMalloc(&b->d_block, total) != cudaSuccess || cudaMalloc(&b->d_desc, table_bytes) != cudaSuccess ||
-      cudaMalloc(&b->d_bar, 4 * sizeof(unsigned int)) != cudaSuccess) {
+      cudaMalloc(&b->d_bar, 4 * sizeof(unsigned long long)) != cudaSuccess) {
     cudaGetLastError();
     pme_batch_destroy(b);
     return fail(PME_ENOMEM, "batch: device allocation failed");
@@ -750,9 +849,12 @@ int pme_batch_create(const pme_system_desc* systems, int nsys, void* stream, pme
   b->d_prefix = (int*)((char*)b->d_desc + align256(sizeof(SysDesc) * nsys));
   b->d_status = (int*)(b->d_bar + 2);
   e = cudaMemset(b->d_block, 0, total);
-  if (e == cudaSuccess) e = cudaMemset(b->d_bar, 0, 4 * sizeof(unsigned int));
+  if (e == cudaSuccess) e = cudaMemset(b->d_bar, 0, 4 * sizeof(unsigned long long));
   for (int i = 0; i < nsys && e == cudaSuccess; i++) {
     b->st[i].carve(b->d_block + off[i]);
+    b->st[i].bins = (int*)(b->d_block + boff[i]);
+    b->st[i].atom_cap = std::max(systems[i].natom, 1);
+    b->st[i].bin_cap = SystemState::cap_for(b->st[i].atom_cap, b->st[i].nbins());
     e = b->st[i].upload_tables();
   }
   if (e != cudaSuccess) {
@@ -828,6 +930,7 @@ int pme_batch_eval(pme_batch* b) {
   a.nsys = (int)b->desc.size();
   a.prefix = b->d_prefix;
   for (int p = 0; p < kPhases; p++) a.total[p] = b->total[p];
+  a.nbar = fused_barriers(a.total);
   a.bar = b->d_bar;
   a.status = b->d_status;
   a.spin_limit = b->spin_limit;

@@ -45,10 +45,18 @@ struct FftPlan1D {
 };
 
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
-  return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+  return make_float2(__fmaf_rn(a.x, b.x, -__fmul_rn(a.y, b.y)), __fmaf_rn(a.x, b.y, __fmul_rn(a.y, b.x)));
 }
-__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) {
+  return make_float2(__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y));
+}
+__device__ __forceinline__ float2 csub(float2 a, float2 b) {
+  return make_float2(__fsub_rn(a.x, b.x), __fsub_rn(a.y, b.y));
+}
+// a + s b with one rounding per component (explicit FMA)
+__device__ __forceinline__ float2 cfma(float s, float2 b, float2 a) {
+  return make_float2(__fmaf_rn(s, b.x, a.x), __fmaf_rn(s, b.y, a.y));
+}
 // s * i * a for s = +1 / -1:  i (x + i y) = -y + i x
 __device__ __forceinline__ float2 cmul_si(float2 a, bool inv) {
   return inv ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
@@ -75,11 +83,11 @@ template <> __device__ __forceinline__ void dft_small<4>(float2* v, bool inv) {
 template <> __device__ __forceinline__ void dft_small<3>(float2* v, bool inv) {
   const float h = 0.866025403784438646763723f;   // sin(2 pi/3)
   float2 s = cadd(v[1], v[2]), d = csub(v[1], v[2]);
-  float2 m = make_float2(v[0].x - 0.5f * s.x, v[0].y - 0.5f * s.y);
+  float2 m = cfma(-0.5f, s, v[0]);
   float2 jd = cmul_si(d, inv);                    // forward: -i d
   v[0] = cadd(v[0], s);
-  v[1] = make_float2(m.x + h * jd.x, m.y + h * jd.y);
-  v[2] = make_float2(m.x - h * jd.x, m.y - h * jd.y);
+  v[1] = cfma(h, jd, m);
+  v[2] = cfma(-h, jd, m);
 }
 
 template <> __device__ __forceinline__ void dft_small<5>(float2* v, bool inv) {
@@ -90,45 +98,45 @@ template <> __device__ __forceinline__ void dft_small<5>(float2* v, bool inv) {
   float2 a1 = cadd(v[1], v[4]), b1 = csub(v[1], v[4]);
   float2 a2 = cadd(v[2], v[3]), b2 = csub(v[2], v[3]);
   float2 x0 = v[0];
-  float2 r1 = make_float2(x0.x + c1 * a1.x + c2 * a2.x, x0.y + c1 * a1.y + c2 * a2.y);
-  float2 r2 = make_float2(x0.x + c2 * a1.x + c1 * a2.x, x0.y + c2 * a1.y + c1 * a2.y);
-  float2 t1 = make_float2(s1 * b1.x + s2 * b2.x, s1 * b1.y + s2 * b2.y);
-  float2 t2 = make_float2(s2 * b1.x - s1 * b2.x, s2 * b1.y - s1 * b2.y);
+  float2 r1 = cfma(c2, a2, cfma(c1, a1, x0));
+  float2 r2 = cfma(c1, a2, cfma(c2, a1, x0));
+  float2 t1 = cfma(s2, b2, make_float2(__fmul_rn(s1, b1.x), __fmul_rn(s1, b1.y)));
+  float2 t2 = cfma(-s1, b2, make_float2(__fmul_rn(s2, b1.x), __fmul_rn(s2, b1.y)));
   float2 j1 = cmul_si(t1, inv), j2 = cmul_si(t2, inv);   // forward: -i t
-  v[0] = make_float2(x0.x + a1.x + a2.x, x0.y + a1.y + a2.y);
+  v[0] = cadd(cadd(x0, a1), a2);
   v[1] = cadd(r1, j1);
   v[4] = csub(r1, j1);
   v[2] = cadd(r2, j2);
   v[3] = csub(r2, j2);
 }
 
-// Thread placement inside a tile: line t = tid mod tx, butterfly lane y = tid div tx (lanes
-// 0..ny-1; threads beyond tx*ny idle during stages).
+// Thread placement inside a tile: line t = tid mod nlines, butterfly lane y = tid div nlines
+// (lanes 0..ny-1; threads beyond nlines*ny idle during stages).
 struct TileLane {
   int t, y, ny;
-  __device__ __forceinline__ TileLane(int tid, int nthreads, int tx) {
-    t = tid % tx;
-    y = tid / tx;
-    ny = nthreads / tx;
+  __device__ __forceinline__ TileLane(int tid, int nthreads, int nlines) {
+    t = tid % nlines;
+    y = tid / nlines;
+    ny = nthreads / nlines;
   }
   __device__ __forceinline__ bool active() const { return y < ny; }
 };
 
-// One Stockham stage over all lines of the tile.
+// One Stockham stage over all lines of the tile; element e of line t lives at e*es + t*ls.
 template <int R>
 __device__ __forceinline__ void fft_stage(const float2* __restrict__ in, float2* __restrict__ out,
-                                          int L, int Ns, const FastDiv& nsd, int ld,
+                                          int L, int Ns, const FastDiv& nsd, int es, int ls,
                                           const TileLane& ln, const float2* tw, bool inv) {
   const int nb = L / R;
   const int tstride = L / (Ns * R);
-  const int t = ln.t;
+  const int lo = ln.t * ls;
   if (!ln.active()) return;
   for (int j = ln.y; j < nb; j += ln.ny) {
     const int blk = fdiv(j, nsd);
     const int k = j - blk * Ns;
     float2 v[R];
 #pragma unroll
-    for (int r = 0; r < R; r++) v[r] = in[(j + r * nb) * ld + t];
+    for (int r = 0; r < R; r++) v[r] = in[(j + r * nb) * es + lo];
 #pragma unroll
     for (int r = 1; r < R; r++) {
       float2 w = tw[r * k * tstride];
@@ -138,15 +146,15 @@ __device__ __forceinline__ void fft_stage(const float2* __restrict__ in, float2*
     dft_small<R>(v, inv);
     const int base = blk * Ns * R + k;
 #pragma unroll
-    for (int u = 0; u < R; u++) out[(base + u * Ns) * ld + t] = v[u];
+    for (int u = 0; u < R; u++) out[(base + u * Ns) * es + lo] = v[u];
   }
 }
 
-// Full transform of the tile held in buf0; returns the buffer that holds the result (buf0 or
-// buf1).  Every thread of the CTA must call it; it synchronises between stages and before
-// returning.
+// Full transform of every line of the tile held in buf0 (element stride es, line stride ls);
+// returns the buffer that holds the result (buf0 or buf1).  Every thread of the CTA must call
+// it; it synchronises between stages and before returning.
 __device__ __forceinline__ float2* fft_tile(float2* buf0, float2* buf1, const FftPlan1D& plan,
-                                            int ld, const TileLane& ln, const float2* tw,
+                                            int es, int ls, const TileLane& ln, const float2* tw,
                                             bool inv) {
   float2* src = buf0;
   float2* dst = buf1;
@@ -156,10 +164,10 @@ __device__ __forceinline__ float2* fft_tile(float2* buf0, float2* buf1, const Ff
     const int R = plan.radix[s];
     const FastDiv nsd = plan.ns_div[s];
     switch (R) {
-      case 4: fft_stage<4>(src, dst, L, Ns, nsd, ld, ln, tw, inv); break;
-      case 2: fft_stage<2>(src, dst, L, Ns, nsd, ld, ln, tw, inv); break;
-      case 3: fft_stage<3>(src, dst, L, Ns, nsd, ld, ln, tw, inv); break;
-      case 5: fft_stage<5>(src, dst, L, Ns, nsd, ld, ln, tw, inv); break;
+      case 4: fft_stage<4>(src, dst, L, Ns, nsd, es, ls, ln, tw, inv); break;
+      case 2: fft_stage<2>(src, dst, L, Ns, nsd, es, ls, ln, tw, inv); break;
+      case 3: fft_stage<3>(src, dst, L, Ns, nsd, es, ls, ln, tw, inv); break;
+      case 5: fft_stage<5>(src, dst, L, Ns, nsd, es, ls, ln, tw, inv); break;
       default: break;
     }
     __syncthreads();

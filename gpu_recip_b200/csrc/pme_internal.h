@@ -24,10 +24,11 @@ struct FusedArgs {
   int nsys;
   const int* prefix;
   int total[kPhases];
-  unsigned int* bar;         // [arrival count, generation], zero-initialised
+  unsigned long long* bar;   // [arrival counter, counter value at launch start], zero-initialised
   int* status;               // kStatus*; sticky until cleared by the host
   unsigned int spin_limit;   // barrier polls before giving up
   int inject;                // 1: CTA 0 leaves before the first barrier (failure-detection test)
+  int nbar;                  // grid barriers per launch (non-empty phases - 1)
   unsigned long long* trace; // optional: [cta][phase][begin, end] %globaltimer stamps
   int trace_ctas;            // CTAs recorded (rows of trace)
 };
@@ -37,6 +38,7 @@ cudaError_t configure_kernels(size_t* max_dyn_smem);
 size_t spread_smem(int order);
 size_t fused_smem_bytes(const SysDesc& d);
 void fused_tile_counts(const SysDesc& d, int* counts);
+int fused_barriers(const int* total);
 
 cudaError_t staged_spread(const SysDesc& d, cudaStream_t s);
 cudaError_t staged_self(const SysDesc& d, cudaStream_t s);

@@ -45,15 +45,13 @@ __global__ void __launch_bounds__(kThreads) k_spread(SysDesc p) {
 
 __global__ void __launch_bounds__(kThreads) k_self(SysDesc p) {
   __shared__ SysDesc d;
-  __shared__ double red[32];
+  __shared__ long long red[32];
   load_desc(d, p);
-  double q2[1] = {0.0};
-  for (int i = blockIdx.x * kThreads + threadIdx.x; i < d.natom; i += gridDim.x * kThreads) {
-    const double q = (double)__ldg(&d.xyzq[i]).w;
-    q2[0] += q * q;
-  }
-  block_sum<1>(q2, red);
-  if (threadIdx.x == 0) acc_add(d.acc, kAccQ2, q2[0], kQ2Scale);
+  long long q2 = 0;
+  for (int i = blockIdx.x * kThreads + threadIdx.x; i < d.natom; i += gridDim.x * kThreads)
+    q2 += q2_fixed(__ldg(&d.xyzq[i]).w);
+  const long long sum = block_sum_ll(q2, red);
+  if (threadIdx.x == 0 && sum != 0) atomicAdd((unsigned long long*)&d.acc[kAccQ2], (unsigned long long)sum);
 }
 
 __global__ void __launch_bounds__(kThreads) k_ktab(SysDesc p) {
@@ -76,11 +74,18 @@ __global__ void __launch_bounds__(kThreads) k_x_inv(SysDesc p) {
   x_inv_tile(d, blockIdx.x, smem);
 }
 
-__global__ void __launch_bounds__(kThreads) k_c2c(SysDesc p, int axis, int mode) {
+__global__ void __launch_bounds__(kThreads) k_ypass(SysDesc p, int mode) {
   __shared__ SysDesc d;
   extern __shared__ float2 smem[];
   load_desc(d, p);
-  c2c_tile(d, axis, mode, blockIdx.x, smem);
+  y_tile(d, mode, blockIdx.x, smem);
+}
+
+__global__ void __launch_bounds__(kThreads) k_zpass(SysDesc p, int mode) {
+  __shared__ SysDesc d;
+  extern __shared__ float2 smem[];
+  load_desc(d, p);
+  z_tile(d, mode, blockIdx.x, smem);
 }
 
 __global__ void __launch_bounds__(kThreads) k_gather(SysDesc p) {
@@ -115,30 +120,42 @@ __device__ __forceinline__ void trace_mark(const FusedArgs& a, int ph, int which
     a.trace[((size_t)blockIdx.x * kPhases + ph) * 2 + which] = globaltimer();
 }
 
-__device__ bool grid_barrier(unsigned int* bar, int* status, unsigned int spin_limit) {
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ void red_release_add_u64(unsigned long long* p, unsigned long long v) {
+  asm volatile("red.release.gpu.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// Grid barrier k of a launch: a monotonic 64-bit arrival counter.  Every CTA adds 1 with release
+// semantics and waits (acquire) until the counter reaches base + (k+1) * gridDim.x, where base is
+// the counter value at launch start (bar[1], advanced once per launch by CTA 0 after barrier 0,
+// when every CTA has read it).  Waits are bounded: after spin_limit polls the CTA records
+// kStatusBarrierTimeout in *status and the kernel returns (no trap, no hang).
+__device__ bool grid_barrier(unsigned long long* bar, unsigned long long base, int k, int nbar,
+                             int* status, unsigned int spin_limit) {
   __shared__ int ok;
   __syncthreads();
   if (threadIdx.x == 0) {
-    const unsigned int gen = ld_acquire(&bar[1]);
-    __threadfence();
-    const unsigned int arrived = atomicAdd(&bar[0], 1u);
+    const unsigned long long target = base + (unsigned long long)(k + 1) * gridDim.x;
+    red_release_add_u64(&bar[0], 1ull);
     int good = 1;
-    if (arrived == gridDim.x - 1) {
-      atomicExch(&bar[0], 0u);
-      __threadfence();
-      atomicAdd(&bar[1], 1u);
-    } else {
-      unsigned int it = 0;
-      while (ld_acquire(&bar[1]) == gen) {
-        if (++it > spin_limit || ld_volatile(status) != 0) {
-          atomicCAS(status, 0, kStatusBarrierTimeout);
-          good = 0;
-          break;
-        }
-        __nanosleep(64);
+    unsigned int it = 0;
+    while (ld_acquire_u64(&bar[0]) < target) {
+      if (++it > spin_limit || ld_volatile(status) != 0) {
+        atomicCAS(status, 0, kStatusBarrierTimeout);
+        good = 0;
+        break;
       }
+      if (it > 64) __nanosleep(32);
     }
-    __threadfence();
+    if (good && k == 0 && blockIdx.x == 0) {
+      bar[1] = base + (unsigned long long)nbar * gridDim.x;
+      bar[3] = bar[3] + 1ull;   // launch counter (bin parity); every CTA read it before barrier 0
+    }
     ok = good;
   }
   __syncthreads();
@@ -158,12 +175,20 @@ __global__ void __launch_bounds__(kThreads) k_fused(FusedArgs a) {
   __shared__ SysDesc d;
   __shared__ int cur;
   extern __shared__ float2 smem[];
-  if (threadIdx.x == 0) cur = -1;
+  __shared__ unsigned long long base;
+  __shared__ int parity;
+  if (threadIdx.x == 0) {
+    cur = -1;
+    base = ld_acquire_u64(&a.bar[1]);
+    parity = (int)(ld_acquire_u64(&a.bar[3]) & 1ull);
+  }
   // a sticky error from an earlier interrupted evaluation: do nothing until the host clears it
   if (ld_volatile(a.status) != kStatusOk) return;
   if (a.table == nullptr) load_desc(d, a.single);
   __syncthreads();
+  int k = 0;   // barriers passed
   for (int ph = 0; ph < kPhases; ph++) {
+    if (a.total[ph] == 0) continue;
     const int* prefix = a.prefix ? a.prefix + ph * (a.nsys + 1) : nullptr;
     trace_mark(a, ph, 0);
     for (int t = blockIdx.x; t < a.total[ph]; t += gridDim.x) {
@@ -179,29 +204,39 @@ __global__ void __launch_bounds__(kThreads) k_fused(FusedArgs a) {
       }
       switch (ph) {
         case 0:
-          if (local < tiles_spread(d)) spread_dispatch(d, local, smem);
+          if (local < tiles_bin(d)) bin_tile(d, local, parity, (long long*)smem);
           else ktab_tile(d);
           break;
-        case 1: x_fwd_tile(d, local, smem, true); break;
-        case 2: c2c_tile(d, 1, 0, local, smem); break;
-        case 3: c2c_tile(d, 2, 2, local, smem); break;
-        case 4:
-          if (local < tiles_ypass(d)) c2c_tile(d, 1, 1, local, smem);
+        case 1: spread_x_dispatch(d, local, parity, (char*)smem); break;
+        case 2:
+          if (d.plane) plane_tile(d, local, smem);
+          else y_tile(d, 0, local, smem);
+          break;
+        case 3: z_tile(d, 2, local, smem); break;
+        case 4: y_tile(d, 1, local, smem); break;
+        case 5:
+          if (local < tiles_xpass(d)) x_inv_tile(d, local, smem);
           else if (threadIdx.x == 0) finalize_system(d, true, true);
           break;
-        case 5: x_inv_tile(d, local, smem); break;
         default: gather_dispatch(d, local); break;
       }
       __syncthreads();
     }
     trace_mark(a, ph, 1);
-    if (a.inject == 1 && ph == 0 && blockIdx.x == 0) return;
-    if (ph + 1 < kPhases && !grid_barrier(a.bar, a.status, a.spin_limit)) return;
+    if (a.inject == 1 && k == 0 && blockIdx.x == 0) return;
+    if (k < a.nbar) {
+      if (!grid_barrier(a.bar, base, k, a.nbar, a.status, a.spin_limit)) return;
+      k++;
+    }
   }
 }
 
 // ------------------------------- host launchers ----------------------------------------------
-static size_t staged_fft_smem(int L, int tx) { return tile_smem_bytes(L, tx) + 32 * 7 * sizeof(double); }
+static size_t staged_fft_smem(int L, int tx) { return tile_smem_bytes(L, tx) + 32 * 7 * sizeof(long long); }
+// z tiles also stage the y and z influence tables
+static size_t staged_z_smem(const SysDesc& d) {
+  return staged_fft_smem(d.g.nz, d.tx_z) + ktab_smem_bytes(d.g.ny, d.g.nz);
+}
 
 size_t spread_smem(int order) {
   switch (order) {
@@ -212,23 +247,28 @@ size_t spread_smem(int order) {
 }
 
 size_t fused_smem_bytes(const SysDesc& d) {
-  size_t m = spread_smem(d.order);
-  const size_t a = staged_fft_smem(d.g.nx, d.tx_rows), b = staged_fft_smem(d.g.ny, d.tx_y),
-               c = staged_fft_smem(d.g.nz, d.tx_z);
-  m = m > a ? m : a;
-  m = m > b ? m : b;
-  m = m > c ? m : c;
+  size_t m = 32 * sizeof(long long);
+  size_t c[5] = {staged_fft_smem(d.g.nx, d.tx_rows), staged_fft_smem(d.g.ny, d.tx_y),
+                 staged_z_smem(d), d.plane ? plane_smem_bytes(d.g.ny, d.g.nz) : 0,
+                 spread_x_smem_bytes(d.g.nx, d.bry * d.brz)};
+  for (size_t v : c) m = m > v ? m : v;
   return m;
 }
 
 void fused_tile_counts(const SysDesc& d, int* counts) {
-  counts[0] = tiles_spread(d) + 1;
-  counts[1] = tiles_xpass(d);
-  counts[2] = tiles_ypass(d);
-  counts[3] = tiles_zpass(d);
-  counts[4] = tiles_ypass(d) + 1;
-  counts[5] = tiles_xpass(d);
+  counts[0] = tiles_bin(d) + 1;
+  counts[1] = tiles_blocks(d);
+  counts[2] = d.plane ? tiles_plane(d) : tiles_ypass(d);
+  counts[3] = d.plane ? 0 : tiles_zpass(d);
+  counts[4] = d.plane ? 0 : tiles_ypass(d);
+  counts[5] = tiles_xpass(d) + 1;
   counts[6] = tiles_gather(d);
+}
+
+int fused_barriers(const int* total) {
+  int nonempty = 0;
+  for (int p = 0; p < kPhases; p++) nonempty += total[p] > 0 ? 1 : 0;
+  return nonempty > 0 ? nonempty - 1 : 0;
 }
 
 cudaError_t staged_spread(const SysDesc& d, cudaStream_t s) {
@@ -252,9 +292,9 @@ cudaError_t staged_r2c(const SysDesc& d, bool zero_accum, cudaStream_t s) {
   k_x_fwd<<<tiles_xpass(d), kThreads, staged_fft_smem(d.g.nx, d.tx_rows), s>>>(d, zero_accum ? 1 : 0);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  k_c2c<<<tiles_ypass(d), kThreads, staged_fft_smem(d.g.ny, d.tx_y), s>>>(d, 1, 0);
+  k_ypass<<<tiles_ypass(d), kThreads, staged_fft_smem(d.g.ny, d.tx_y), s>>>(d, 0);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  k_c2c<<<tiles_zpass(d), kThreads, staged_fft_smem(d.g.nz, d.tx_z), s>>>(d, 2, 0);
+  k_zpass<<<tiles_zpass(d), kThreads, staged_z_smem(d), s>>>(d, 0);
   return cudaGetLastError();
 }
 
@@ -262,17 +302,17 @@ cudaError_t staged_solve(const SysDesc& d, cudaStream_t s) {
   k_ktab<<<1, kThreads, 0, s>>>(d);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  k_c2c<<<tiles_zpass(d), kThreads, staged_fft_smem(d.g.nz, d.tx_z), s>>>(d, 2, 3);
+  k_zpass<<<tiles_zpass(d), kThreads, staged_z_smem(d), s>>>(d, 3);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   k_finalize<<<1, 32, 0, s>>>(d, 1, 0);
   return cudaGetLastError();
 }
 
 cudaError_t staged_c2r(const SysDesc& d, cudaStream_t s) {
-  k_c2c<<<tiles_zpass(d), kThreads, staged_fft_smem(d.g.nz, d.tx_z), s>>>(d, 2, 1);
+  k_zpass<<<tiles_zpass(d), kThreads, staged_z_smem(d), s>>>(d, 1);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  k_c2c<<<tiles_ypass(d), kThreads, staged_fft_smem(d.g.ny, d.tx_y), s>>>(d, 1, 1);
+  k_ypass<<<tiles_ypass(d), kThreads, staged_fft_smem(d.g.ny, d.tx_y), s>>>(d, 1);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   k_x_inv<<<tiles_xpass(d), kThreads, staged_fft_smem(d.g.nx, d.tx_rows), s>>>(d);
   return cudaGetLastError();
@@ -322,7 +362,8 @@ cudaError_t configure_kernels(size_t* max_dyn_smem) {
   if ((e = opt_in_smem(k_spread, optin)) != cudaSuccess) return e;
   if ((e = opt_in_smem(k_x_fwd, optin)) != cudaSuccess) return e;
   if ((e = opt_in_smem(k_x_inv, optin)) != cudaSuccess) return e;
-  if ((e = opt_in_smem(k_c2c, optin)) != cudaSuccess) return e;
+  if ((e = opt_in_smem(k_ypass, optin)) != cudaSuccess) return e;
+  if ((e = opt_in_smem(k_zpass, optin)) != cudaSuccess) return e;
   if ((e = opt_in_smem(k_fused, optin)) != cudaSuccess) return e;
   cudaFuncAttributes fa;
   if ((e = cudaFuncGetAttributes(&fa, k_fused)) != cudaSuccess) return e;

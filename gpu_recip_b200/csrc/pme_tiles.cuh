@@ -37,6 +37,7 @@ struct SysDesc {
   int natom;
   double fac;                // pi^2 / kappa^2
   double piv_inv;            // 1 / (pi V)
+  float fac_f, piv_inv_f;    // the same, FP32
   double rxd, ryd, rzd;      // reciprocal box diagonal, FP64
   int calc_ev;               // energy + virial in the solve
   int calc_self;             // self energy in the spread phase
@@ -54,14 +55,37 @@ struct SysDesc {
   long long* acc;            // kAccCount fixed-point accumulators
   double* ev;                // kEvCount record
   int tx_rows, tx_y, tx_z;   // lines per tile of the x, y, z passes
+  int plane;                 // 1: the fused path runs y, z and the solve as whole-plane tiles
+  // Atom bins of the fused path: bin (by, bz) holds the atoms whose stencil origin (iy0, iz0)
+  // lies in row block [by*bry, by*bry+bry) x [bz*brz, bz*brz+brz); fixed capacity bin_cap per bin,
+  // surplus atoms go to an overflow list.  Counters are double-buffered by launch parity.
+  int bry, brz, nby, nbz;
+  int bin_cap;
+  int* bin_count;            // [2][nby*nbz]
+  int* bin_atoms;            // [nby*nbz][bin_cap]
+  int* ovf_count;            // [2]
+  int* ovf_atoms;            // [natom capacity]
+  unsigned long long* steps; // profiling: %globaltimer at the steps of CTA 0's tiles (or null)
 };
+
+// Profiling stamp of one step of a tile (CTA 0, thread 0 only; no-op when steps is null).
+__device__ __forceinline__ void step_mark(const SysDesc& d, int slot) {
+  if (d.steps != nullptr && blockIdx.x == 0 && threadIdx.x == 0) {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    d.steps[slot] = t;
+  }
+}
 
 constexpr int kSpreadAtomsPerWarp = 8;
 constexpr int kSpreadAtoms = kSpreadAtomsPerWarp * (kThreads / 32);   // atoms per spread tile
 __host__ __device__ inline int tiles_spread(const SysDesc& d) { return (d.natom + kSpreadAtoms - 1) / kSpreadAtoms; }
 __host__ __device__ inline int tiles_xpass(const SysDesc& d) { return (d.g.ny * d.g.nz + d.tx_rows - 1) / d.tx_rows; }
-__host__ __device__ inline int tiles_ypass(const SysDesc& d) { return ((d.g.hx + d.tx_y - 1) / d.tx_y) * d.g.nz; }
-__host__ __device__ inline int tiles_zpass(const SysDesc& d) { return ((d.g.hx + d.tx_z - 1) / d.tx_z) * d.g.ny; }
+__host__ __device__ inline int tiles_ypass(const SysDesc& d) { return (d.g.hx * d.g.nz + d.tx_y - 1) / d.tx_y; }
+__host__ __device__ inline int tiles_zpass(const SysDesc& d) { return ((d.g.ny + d.tx_z - 1) / d.tx_z) * d.g.hx; }
+__host__ __device__ inline int tiles_plane(const SysDesc& d) { return d.g.hx; }
+__host__ __device__ inline int tiles_bin(const SysDesc& d) { return (d.natom + kThreads - 1) / kThreads; }
+__host__ __device__ inline int tiles_blocks(const SysDesc& d) { return d.nby * d.nbz; }
 __host__ __device__ inline int tiles_gather(const SysDesc& d) { return (d.natom + 31) / 32; }
 __host__ inline size_t tile_smem_bytes(int L, int tx) {
   return sizeof(float2) * ((size_t)L + 2 * (size_t)L * (tx + 1));
@@ -99,6 +123,25 @@ __device__ __forceinline__ void acc_add(long long* acc, int slot, double v, doub
   atomicAdd((unsigned long long*)&acc[slot], (unsigned long long)__double2ll_rn(v * scale));
 }
 
+// Block sum of one int64 per thread; the result is valid in thread 0.  `scratch`: 32 int64.
+__device__ __forceinline__ long long block_sum_ll(long long v, long long* scratch) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int off = 16; off >= 1; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+  __syncthreads();
+  if (lane == 0) scratch[warp] = v;
+  __syncthreads();
+  long long s = 0;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < nw; w++) s += scratch[w];
+  return s;
+}
+
+// q^2 of one atom in the sum-of-squares fixed point (one rounding per atom).
+__device__ __forceinline__ long long q2_fixed(float q) {
+  return __double2ll_rn((double)q * (double)q * kQ2Scale);
+}
+
 // ---------------------------------------------------------------------------------------------
 // Spread tile: kSpreadAtoms atoms; warp w spreads atoms [8w, 8w+8) of the tile.  Lanes 0..7 each
 // compute one atom's stencil origin and weights (q folded into x), then the warp covers the
@@ -116,12 +159,12 @@ template <int P>
 __device__ __forceinline__ void spread_tile(const SysDesc& d, int tile, void* smem) {
   constexpr int APW = kSpreadAtomsPerWarp;
   SplineAtom<P>* sh = (SplineAtom<P>*)smem;
-  double* red = (double*)((char*)smem + ((sizeof(SplineAtom<P>) * kSpreadAtoms + 7) / 8) * 8);
+  long long* red = (long long*)((char*)smem + ((sizeof(SplineAtom<P>) * kSpreadAtoms + 7) / 8) * 8);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const Geom& g = d.g;
   const int base = tile * kSpreadAtoms + warp * APW;
   const int cnt = max(0, min(APW, d.natom - base));
-  double q2[1] = {0.0};
+  long long q2 = 0;
   if (lane < cnt) {
     const float4 a = __ldg(&d.xyzq[base + lane]);
     SplineAtom<P>& s = sh[warp * APW + lane];
@@ -138,7 +181,7 @@ __device__ __forceinline__ void spread_tile(const SysDesc& d, int tile, void* sm
     bspline<P>(uz, th, nullptr);
 #pragma unroll
     for (int i = 0; i < P; i++) s.tz[i] = th[i];
-    q2[0] = (double)a.w * (double)a.w;
+    q2 = q2_fixed(a.w);
   }
   __syncwarp();
   constexpr int P3 = P * P * P;
@@ -155,8 +198,8 @@ __device__ __forceinline__ void spread_tile(const SysDesc& d, int tile, void* sm
     atomicAdd(&accum[x + (size_t)nx * (y + (size_t)ny * z)], (unsigned long long)v);
   }
   if (d.calc_self) {
-    block_sum<1>(q2, red);
-    if (threadIdx.x == 0 && d.natom > 0) acc_add(d.acc, kAccQ2, q2[0], kQ2Scale);
+    const long long sum = block_sum_ll(q2, red);
+    if (threadIdx.x == 0 && sum != 0) atomicAdd((unsigned long long*)&d.acc[kAccQ2], (unsigned long long)sum);
   }
   __syncthreads();
 }
@@ -164,6 +207,14 @@ __device__ __forceinline__ void spread_tile(const SysDesc& d, int tile, void* sm
 template <int P>
 __host__ inline size_t spread_smem_bytes() {
   return ((sizeof(SplineAtom<P>) * kSpreadAtoms + 7) / 8) * 8 + 32 * sizeof(double);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Half-complex grid layout: [kx][z][y] (y fastest), so y-lines are contiguous and each kx plane is
+// one contiguous ny*nz block.
+// ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ size_t cidx(const Geom& g, int kx, int z, int y) {
+  return ((size_t)kx * g.nz + z) * g.ny + y;
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -182,7 +233,7 @@ __device__ __forceinline__ void x_fwd_tile(const SysDesc& d, int tile, float2* s
   const int nrows = g.ny * g.nz, row0 = tile * tx;
   for (int i = tid; i < L; i += kThreads) tw[i] = __ldg(&d.tw[plan.tw_off + i]);
   const unsigned long long* __restrict__ src = d.accum + (size_t)row0 * L;
-  const int nvalid = min(tx, nrows - row0) * L;   // rows of this tile inside the grid
+  const int nvalid = min(tx, nrows - row0) * L;   // elements of this tile's rows inside the grid
 #pragma unroll 4
   for (int idx = tid; idx < L * tx; idx += kThreads) {
     const int t = fdiv(idx, plan.n_div), e = idx - t * L;
@@ -195,12 +246,15 @@ __device__ __forceinline__ void x_fwd_tile(const SysDesc& d, int tile, float2* s
   }
   __syncthreads();
   TileLane ln(tid, kThreads, tx);
-  float2* res = fft_tile(b0, b1, plan, ld, ln, tw, false);
+  float2* res = fft_tile(b0, b1, plan, ld, 1, ln, tw, false);
   const int hx = g.hx;
-  const FastDiv hxd = make_fastdiv(hx);
+  const FastDiv txd = make_fastdiv(tx), nyd = d.py.n_div;
   for (int idx = tid; idx < hx * tx; idx += kThreads) {
-    const int t = fdiv(idx, hxd), k = idx - t * hx, row = row0 + t;
-    if (row < nrows) __stcg(&d.cgrid[(size_t)row * hx + k], res[k * ld + t]);
+    const int k = fdiv(idx, txd), t = idx - k * tx, row = row0 + t;
+    if (row < nrows) {
+      const int z = fdiv(row, nyd), y = row - z * g.ny;
+      __stcg(&d.cgrid[cidx(g, k, z, y)], res[k * ld + t]);
+    }
   }
   __syncthreads();
 }
@@ -216,18 +270,21 @@ __device__ __forceinline__ void x_inv_tile(const SysDesc& d, int tile, float2* s
   float2* b1 = b0 + L * ld;
   const int tid = threadIdx.x;
   const int nrows = g.ny * g.nz, row0 = tile * tx;
-  const FastDiv hxd = make_fastdiv(hx);
+  const FastDiv txd = make_fastdiv(tx), nyd = d.py.n_div;
   for (int i = tid; i < L; i += kThreads) tw[i] = __ldg(&d.tw[plan.tw_off + i]);
   for (int idx = tid; idx < hx * tx; idx += kThreads) {
-    const int t = fdiv(idx, hxd), k = idx - t * hx, row = row0 + t;
+    const int k = fdiv(idx, txd), t = idx - k * tx, row = row0 + t;
     float2 v = make_float2(0.0f, 0.0f);
-    if (row < nrows) v = __ldcg(&d.cgrid[(size_t)row * hx + k]);
+    if (row < nrows) {
+      const int z = fdiv(row, nyd), y = row - z * g.ny;
+      v = __ldcg(&d.cgrid[cidx(g, k, z, y)]);
+    }
     b0[k * ld + t] = v;
     if (k >= 1 && L - k >= hx) b0[(L - k) * ld + t] = make_float2(v.x, -v.y);
   }
   __syncthreads();
   TileLane ln(tid, kThreads, tx);
-  float2* res = fft_tile(b0, b1, plan, ld, ln, tw, true);
+  float2* res = fft_tile(b0, b1, plan, ld, 1, ln, tw, true);
   for (int idx = tid; idx < L * tx; idx += kThreads) {
     const int t = fdiv(idx, plan.n_div), e = idx - t * L, row = row0 + t;
     if (row < nrows) __stcg(&d.rgrid[(size_t)row * L + e], res[e * ld + t].x);
@@ -258,130 +315,504 @@ __device__ __forceinline__ void ktab_tile(const SysDesc& d) {
   }
 }
 
-struct KTerm {
-  double eterm, m1, m2, m3, msq;
+// Solve terms of one stored k.  The mirror -k that the reference adds for kx >= 1
+// (CudaPMERecip.cu:708-742) has the same |m|^2 and the same eterm (the per-axis factors are
+// even in m); its off-diagonal products m_i m_j change sign unless one of the two components sits
+// at k = 0 or on an even-length Nyquist plane, where the mirrored index maps onto itself.
+// Influence-table view for one tile: the tile's fixed kx values in registers, the y and z tables
+// staged in shared memory, all rounded once from the FP64 tables to FP32.
+struct KTab {
+  float m1, A1;
+  const float* my;   // [ny] mhat_y
+  const float* mz;   // [nz] mhat_z
+  const float* Ay;   // [ny] A_y
+  const float* Az;   // [nz] A_z
 };
 
-__device__ __forceinline__ KTerm kterm(int kx, int ky, int kz, const SysDesc& d) {
+__host__ __device__ inline size_t ktab_smem_bytes(int ny, int nz) { return 2 * sizeof(float) * ((size_t)ny + nz); }
+
+// Stage mhat and A for y and z into `sm` (2 (ny + nz) floats) and load kx's.  The caller
+// synchronises before use.
+__device__ __forceinline__ KTab stage_ktab(const SysDesc& d, int kx, float* sm) {
   const Geom& g = d.g;
-  const double* mh = d.ktab;
-  const double* A = d.ktab + g.nx + g.ny + g.nz;
-  KTerm o;
-  o.m1 = __ldcg(&mh[kx]);
-  o.m2 = __ldcg(&mh[g.nx + ky]);
-  o.m3 = __ldcg(&mh[g.nx + g.ny + kz]);
-  o.msq = o.m1 * o.m1 + o.m2 * o.m2 + o.m3 * o.m3;
-  o.eterm = d.piv_inv * __ldcg(&A[kx]) * __ldcg(&A[g.nx + ky]) * __ldcg(&A[g.nx + g.ny + kz]) / o.msq;
-  return o;
+  const int ntot = g.nx + g.ny + g.nz;
+  const int nyz = g.ny + g.nz;
+  for (int i = threadIdx.x; i < nyz; i += kThreads) {
+    sm[i] = (float)__ldcg(&d.ktab[g.nx + i]);
+    sm[nyz + i] = (float)__ldcg(&d.ktab[ntot + g.nx + i]);
+  }
+  KTab t;
+  t.m1 = (float)__ldcg(&d.ktab[kx]);
+  t.A1 = (float)__ldcg(&d.ktab[ntot + kx]);
+  t.my = sm;
+  t.mz = sm + g.ny;
+  t.Ay = sm + nyz;
+  t.Az = sm + nyz + g.ny;
+  return t;
 }
 
-// Energy and virial terms of one k (CudaPMERecip.cu:694-742), FP64:
-// [t, t (v m1 m1 - 1), t v m1 m2, t v m1 m3, t (v m2 m2 - 1), t v m2 m3, t (v m3 m3 - 1)],
-// t = eterm |Q|^2, v = 2 (fac + 1/|m|^2).
-__device__ __forceinline__ void ev_accum(double* acc, const KTerm& k, double q2, double fac) {
-  const double t1 = k.eterm * q2;
-  const double vt = 2.0 * (fac + 1.0 / k.msq);
-  acc[0] += t1;
-  acc[1] += t1 * (vt * k.m1 * k.m1 - 1.0);
-  acc[2] += t1 * vt * k.m1 * k.m2;
-  acc[3] += t1 * vt * k.m1 * k.m3;
-  acc[4] += t1 * (vt * k.m2 * k.m2 - 1.0);
-  acc[5] += t1 * vt * k.m2 * k.m3;
-  acc[6] += t1 * (vt * k.m3 * k.m3 - 1.0);
+// Solve one stored element: Q *= eterm (Q(0) = 0) and, when asked, add its energy and virial
+// terms (CudaPMERecip.cu:694-742) to the fixed-point accumulators `acc`: each term is rounded to
+// an integer number of 2^-32 units once, so the sums are exact and do not depend on how elements
+// are split into tiles or batches.  eterm = piv_inv A_x A_y A_z / |m|^2 from the FP64-built
+// tables; t = eterm |Q|^2, v = 2 (fac + 1/|m|^2); [t, t (v m1 m1 - 1), t v m1 m2, t v m1 m3,
+// t (v m2 m2 - 1), t v m2 m3, t (v m3 m3 - 1)], doubled for kx >= 1 (the mirror -k, which has the
+// same |m|^2 and eterm), with the mirror's off-diagonals multiplied by s_i s_j (s = -1 where the
+// mirror flips m_i, +1 at k = 0 and on an even-length Nyquist plane).
+__device__ __forceinline__ void solve_elem(float2& q, int kx, int ky, int kz, const SysDesc& d,
+                                           const KTab& kt, long long* acc) {
+  const Geom& g = d.g;
+  if (kx == 0 && ky == 0 && kz == 0) {
+    q = make_float2(0.0f, 0.0f);
+    return;
+  }
+  // explicit roundings: the same bits in every kernel this is inlined into
+  const float m1 = kt.m1, m2 = kt.my[ky], m3 = kt.mz[kz];
+  const float inv_msq = __frcp_rn(__fmaf_rn(m3, m3, __fmaf_rn(m2, m2, __fmul_rn(m1, m1))));
+  const float eterm =
+      __fmul_rn(__fmul_rn(__fmul_rn(__fmul_rn(d.piv_inv_f, kt.A1), kt.Ay[ky]), kt.Az[kz]), inv_msq);
+  if (d.calc_ev) {
+    const float q2 = __fmaf_rn(q.y, q.y, __fmul_rn(q.x, q.x));
+    const bool mirror = kx >= 1;
+    const float sx = (2 * kx == g.nx) ? 1.0f : -1.0f;
+    const float sy = (ky == 0 || 2 * ky == g.ny) ? 1.0f : -1.0f;
+    const float sz = (kz == 0 || 2 * kz == g.nz) ? 1.0f : -1.0f;
+    const float t1 = __fmul_rn(__fmul_rn(eterm, q2), (float)kEvScale);
+    const float vt = __fmul_rn(2.0f, __fadd_rn(d.fac_f, inv_msq));
+    const float w = mirror ? 2.0f : 1.0f;
+    const float txy = mirror ? __fadd_rn(1.0f, __fmul_rn(sx, sy)) : 1.0f;
+    const float txz = mirror ? __fadd_rn(1.0f, __fmul_rn(sx, sz)) : 1.0f;
+    const float tyz = mirror ? __fadd_rn(1.0f, __fmul_rn(sy, sz)) : 1.0f;
+    const float wt = __fmul_rn(w, t1);
+    const float tv = __fmul_rn(t1, vt);
+    acc[0] += __float2ll_rn(wt);
+    acc[1] += __float2ll_rn(__fmul_rn(wt, __fmaf_rn(__fmul_rn(vt, m1), m1, -1.0f)));
+    acc[2] += __float2ll_rn(__fmul_rn(__fmul_rn(__fmul_rn(txy, tv), m1), m2));
+    acc[3] += __float2ll_rn(__fmul_rn(__fmul_rn(__fmul_rn(txz, tv), m1), m3));
+    acc[4] += __float2ll_rn(__fmul_rn(wt, __fmaf_rn(__fmul_rn(vt, m2), m2, -1.0f)));
+    acc[5] += __float2ll_rn(__fmul_rn(__fmul_rn(__fmul_rn(tyz, tv), m2), m3));
+    acc[6] += __float2ll_rn(__fmul_rn(wt, __fmaf_rn(__fmul_rn(vt, m3), m3, -1.0f)));
+  }
+  q.x = __fmul_rn(q.x, eterm);
+  q.y = __fmul_rn(q.y, eterm);
 }
 
-// Solve on a z-line tile held in smem (lines = kx0.. at fixed ky, elements = kz).  Every stored k
-// contributes its own term and, for kx >= 1, the term of its mirror -k (the reference's x-mirror
-// doubling, CudaPMERecip.cu:708-742).  Q(0) is zeroed.
-__device__ __forceinline__ void solve_tile(float2* buf, int ld, int tx, const FastDiv& txd, int kx0,
-                                           int ky, const SysDesc& d, double* acc) {
-  const Geom& g = d.g;
-  const int L = g.nz;
-  const double facd = d.fac;
-  for (int idx = threadIdx.x; idx < L * tx; idx += kThreads) {
-    const int e = fdiv(idx, txd), t = idx - e * tx, kx = kx0 + t, kz = e;
-    if (kx >= g.hx) continue;
-    float2 q = buf[e * ld + t];
-    if (kx == 0 && ky == 0 && kz == 0) {
-      buf[e * ld + t] = make_float2(0.0f, 0.0f);
-      continue;
-    }
-    const KTerm k = kterm(kx, ky, kz, d);
-    if (d.calc_ev) {
-      const double q2 = (double)q.x * (double)q.x + (double)q.y * (double)q.y;
-      ev_accum(acc, k, q2, facd);
-      if (kx >= 1) {
-        const int kxs = g.nx - kx, kys = ky == 0 ? 0 : g.ny - ky, kzs = kz == 0 ? 0 : g.nz - kz;
-        const KTerm ks = kterm(kxs, kys, kzs, d);
-        ev_accum(acc, ks, q2, facd);
-      }
-    }
-    const float et = (float)k.eterm;
-    q.x *= et;
-    q.y *= et;
-    buf[e * ld + t] = q;
+// Block-sum 7 int64 partial accumulators and add them to the system's accumulators.
+__device__ __forceinline__ void flush_ev(const SysDesc& d, long long (&acc)[7], long long* red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int off = 16; off >= 1; off >>= 1)
+#pragma unroll
+    for (int c = 0; c < 7; c++) acc[c] += __shfl_down_sync(0xffffffffu, acc[c], off);
+  __syncthreads();
+  if (lane == 0)
+#pragma unroll
+    for (int c = 0; c < 7; c++) red[warp * 7 + c] = acc[c];
+  __syncthreads();
+  if (threadIdx.x < 7) {
+    long long sum = 0;
+    for (int w = 0; w < nw; w++) sum += red[w * 7 + threadIdx.x];
+    atomicAdd((unsigned long long*)&d.acc[kAccE + threadIdx.x], (unsigned long long)sum);
   }
 }
 
-// Complex pass along y (axis 1) or z (axis 2).  A tile is tx consecutive kx at one outer index
-// (z for the y pass, y for the z pass), so each element row of the tile is tx contiguous complex
-// values.  mode: 0 forward, 1 inverse, 2 forward + solve + inverse (z), 3 solve only (z).
-// smem: twiddles, two tile buffers, 32*7 doubles.
-__device__ __forceinline__ void c2c_tile(const SysDesc& d, int axis, int mode, int tile, float2* smem) {
+// y pass: tx_y consecutive y-lines (line = kx nz + z, contiguous ny values).  mode 0 forward,
+// 1 inverse.  smem: twiddles + two tile buffers.
+__device__ __forceinline__ void y_tile(const SysDesc& d, int mode, int tile, float2* smem) {
   const Geom& g = d.g;
-  const FftPlan1D& plan = axis == 1 ? d.py : d.pz;
-  const int tx = axis == 1 ? d.tx_y : d.tx_z;
-  const int L = plan.n, ld = tx + 1;
+  const FftPlan1D& plan = d.py;
+  const int L = g.ny, tx = d.tx_y, ld = tx + 1;
   float2* tw = smem;
   float2* b0 = tw + L;
   float2* b1 = b0 + L * ld;
-  double* red = (double*)(b1 + L * ld);
   const int tid = threadIdx.x;
-  const int tiles_x = (g.hx + tx - 1) / tx;
-  const int outer = tile / tiles_x, tile_x = tile - outer * tiles_x;
-  const int kx0 = tile_x * tx;
-  const FastDiv txd = make_fastdiv(tx);
-  size_t estride, obase;
-  if (axis == 1) {
-    estride = (size_t)g.hx;
-    obase = (size_t)outer * g.hx * g.ny;
-  } else {
-    estride = (size_t)g.hx * g.ny;
-    obase = (size_t)outer * g.hx;
+  const int nlines = g.hx * g.nz, l0 = tile * tx;
+  const int nvalid = min(tx, nlines - l0) * L;
+  float2* __restrict__ base = d.cgrid + (size_t)l0 * L;
+  for (int i = tid; i < L; i += kThreads) tw[i] = __ldg(&d.tw[plan.tw_off + i]);
+#pragma unroll 4
+  for (int idx = tid; idx < L * tx; idx += kThreads) {
+    const int t = fdiv(idx, plan.n_div), e = idx - t * L;
+    b0[e * ld + t] = idx < nvalid ? __ldcg(&base[idx]) : make_float2(0.0f, 0.0f);
   }
+  __syncthreads();
+  TileLane ln(tid, kThreads, tx);
+  float2* res = fft_tile(b0, b1, plan, ld, 1, ln, tw, mode == 1);
+  for (int idx = tid; idx < nvalid; idx += kThreads) {
+    const int t = fdiv(idx, plan.n_div), e = idx - t * L;
+    __stcg(&base[idx], res[e * ld + t]);
+  }
+  __syncthreads();
+}
+
+// z pass: tx_z consecutive y at one kx, all z (element row of the tile = tx contiguous complex).
+// mode: 0 forward, 1 inverse, 2 forward + solve + inverse, 3 solve only.
+// smem: twiddles, two tile buffers, 32*7 int64.
+__device__ __forceinline__ void z_tile(const SysDesc& d, int mode, int tile, float2* smem) {
+  const Geom& g = d.g;
+  const FftPlan1D& plan = d.pz;
+  const int L = g.nz, tx = d.tx_z, ld = tx + 1;
+  float2* tw = smem;
+  float2* b0 = tw + L;
+  float2* b1 = b0 + L * ld;
+  long long* red = (long long*)(b1 + L * ld);
+  float* ksm = (float*)(red + 32 * 7);
+  const int tid = threadIdx.x;
+  const int tpk = (g.ny + tx - 1) / tx;
+  const int kx = tile / tpk, y0 = (tile - kx * tpk) * tx;
+  const int nt = min(tx, g.ny - y0);
+  const FastDiv txd = make_fastdiv(tx);
+  float2* __restrict__ base = d.cgrid + cidx(g, kx, 0, y0);
+  const size_t es = (size_t)g.ny;
   if (mode != 3)
     for (int i = tid; i < L; i += kThreads) tw[i] = __ldg(&d.tw[plan.tw_off + i]);
   for (int idx = tid; idx < L * tx; idx += kThreads) {
-    const int e = fdiv(idx, txd), t = idx - e * tx, kx = kx0 + t;
-    float2 v = make_float2(0.0f, 0.0f);
-    if (kx < g.hx) v = __ldcg(&d.cgrid[obase + e * estride + kx]);
-    b0[e * ld + t] = v;
+    const int e = fdiv(idx, txd), t = idx - e * tx;
+    b0[e * ld + t] = t < nt ? __ldcg(&base[e * es + t]) : make_float2(0.0f, 0.0f);
   }
   __syncthreads();
   TileLane ln(tid, kThreads, tx);
   float2* res = b0;
-  if (mode == 0 || mode == 2) res = fft_tile(b0, b1, plan, ld, ln, tw, false);
-  if (mode == 1) res = fft_tile(b0, b1, plan, ld, ln, tw, true);
+  if (mode == 0 || mode == 2) res = fft_tile(b0, b1, plan, ld, 1, ln, tw, false);
+  if (mode == 1) res = fft_tile(b0, b1, plan, ld, 1, ln, tw, true);
   if (mode == 2 || mode == 3) {
-    double acc[7] = {0, 0, 0, 0, 0, 0, 0};
-    solve_tile(res, ld, tx, txd, kx0, outer, d, acc);
+    const KTab kt = stage_ktab(d, kx, ksm);
     __syncthreads();
-    if (d.calc_ev) {
-      block_sum<7>(acc, red);
-      if (tid == 0)
-#pragma unroll
-        for (int c = 0; c < 7; c++) acc_add(d.acc, kAccE + c, acc[c], kEvScale);
+    long long acc[7] = {0, 0, 0, 0, 0, 0, 0};
+    for (int idx = tid; idx < L * tx; idx += kThreads) {
+      const int e = fdiv(idx, txd), t = idx - e * tx;
+      if (t < nt) solve_elem(res[e * ld + t], kx, y0 + t, e, d, kt, acc);
     }
+    if (d.calc_ev) flush_ev(d, acc, red);
+    __syncthreads();
     if (mode == 2) {
       float2* other = (res == b0) ? b1 : b0;
-      res = fft_tile(res, other, plan, ld, ln, tw, true);
+      res = fft_tile(res, other, plan, ld, 1, ln, tw, true);
     }
   }
   for (int idx = tid; idx < L * tx; idx += kThreads) {
-    const int e = fdiv(idx, txd), t = idx - e * tx, kx = kx0 + t;
-    if (kx < g.hx) __stcg(&d.cgrid[obase + e * estride + kx], res[e * ld + t]);
+    const int e = fdiv(idx, txd), t = idx - e * tx;
+    if (t < nt) __stcg(&base[e * es + t], res[e * ld + t]);
   }
   __syncthreads();
+}
+
+// Whole kx plane (ny x nz, contiguous): y forward, z forward, solve with energy/virial, z inverse,
+// y inverse, all in shared memory (plane held as buf[z * (ny+1) + y]).  Used when the plane fits.
+__host__ __device__ inline size_t plane_smem_bytes(int ny, int nz) {
+  return sizeof(float2) * ((size_t)ny + nz + 2 * (size_t)nz * (ny + 1)) + 32 * 7 * sizeof(long long) +
+         2 * sizeof(float) * ((size_t)ny + nz);
+}
+
+__device__ __forceinline__ void plane_tile(const SysDesc& d, int kx, float2* smem) {
+  const Geom& g = d.g;
+  const int ny = g.ny, nz = g.nz, LD = ny + 1;
+  float2* twy = smem;
+  float2* twz = twy + ny;
+  float2* b0 = twz + nz;
+  float2* b1 = b0 + (size_t)nz * LD;
+  long long* red = (long long*)(b1 + (size_t)nz * LD);
+  float* ksm = (float*)(red + 32 * 7);
+  const int tid = threadIdx.x;
+  float2* __restrict__ base = d.cgrid + cidx(g, kx, 0, 0);
+  step_mark(d, 8);
+  const KTab kt = stage_ktab(d, kx, ksm);
+  for (int i = tid; i < ny; i += kThreads) twy[i] = __ldg(&d.tw[d.py.tw_off + i]);
+  for (int i = tid; i < nz; i += kThreads) twz[i] = __ldg(&d.tw[d.pz.tw_off + i]);
+  const FastDiv nyd = d.py.n_div;
+#pragma unroll 4
+  for (int idx = tid; idx < ny * nz; idx += kThreads) {
+    const int z = fdiv(idx, nyd), y = idx - z * ny;
+    b0[z * LD + y] = __ldcg(&base[idx]);
+  }
+  __syncthreads();
+  step_mark(d, 9);
+  const TileLane lz(tid, kThreads, nz);   // y-FFT: one line per z
+  const TileLane ly(tid, kThreads, ny);   // z-FFT: one line per y
+  float2* r = fft_tile(b0, b1, d.py, 1, LD, lz, twy, false);
+  step_mark(d, 10);
+  float2* o = (r == b0) ? b1 : b0;
+  r = fft_tile(r, o, d.pz, LD, 1, ly, twz, false);
+  step_mark(d, 11);
+  long long acc[7] = {0, 0, 0, 0, 0, 0, 0};
+  for (int idx = tid; idx < ny * nz; idx += kThreads) {
+    const int z = fdiv(idx, nyd), y = idx - z * ny;
+    solve_elem(r[z * LD + y], kx, y, z, d, kt, acc);
+  }
+  if (d.calc_ev) flush_ev(d, acc, red);
+  __syncthreads();
+  step_mark(d, 12);
+  o = (r == b0) ? b1 : b0;
+  r = fft_tile(r, o, d.pz, LD, 1, ly, twz, true);
+  o = (r == b0) ? b1 : b0;
+  r = fft_tile(r, o, d.py, 1, LD, lz, twy, true);
+  step_mark(d, 13);
+  for (int idx = tid; idx < ny * nz; idx += kThreads) {
+    const int z = fdiv(idx, nyd), y = idx - z * ny;
+    __stcg(&base[idx], r[z * LD + y]);
+  }
+  __syncthreads();
+  step_mark(d, 14);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Fused path, phase 0: bin kThreads atoms by the row block of their stencil origin; sum q^2.
+// ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ void bin_tile(const SysDesc& d, int tile, int parity, long long* red) {
+  const Geom& g = d.g;
+  const int i = tile * kThreads + threadIdx.x;
+  const int nbins = d.nby * d.nbz;
+  long long q2 = 0;
+  if (i < d.natom) {
+    const float4 a = __ldg(&d.xyzq[i]);
+    int iy, iz;
+    float u;
+    frac_coord(a.y, g.sy_hi, g.sy_lo, g.ny, iy, u);
+    frac_coord(a.z, g.sz_hi, g.sz_lo, g.nz, iz, u);
+    const int b = iy / d.bry + d.nby * (iz / d.brz);
+    const int slot = atomicAdd(&d.bin_count[parity * nbins + b], 1);
+    if (slot < d.bin_cap) {
+      d.bin_atoms[(size_t)b * d.bin_cap + slot] = i;
+    } else {
+      const int o = atomicAdd(&d.ovf_count[parity], 1);
+      d.ovf_atoms[o] = i;
+    }
+    q2 = q2_fixed(a.w);
+  }
+  if (d.calc_self) {
+    const long long sum = block_sum_ll(q2, red);
+    if (threadIdx.x == 0 && sum != 0) atomicAdd((unsigned long long*)&d.acc[kAccQ2], (unsigned long long)sum);
+  }
+  __syncthreads();
+}
+
+// ---------------------------------------------------------------------------------------------
+// Fused path, phase 1: spread + x forward for one row block (rows y in [Y0, Y0+bry), z in
+// [Z0, Z0+brz), all x).  The block's candidate atoms are those binned in the row blocks whose
+// origins can reach it (origin rows Y0-P+1 .. Y0+bry-1, wrapped), plus the overflow list.  Each
+// contribution that lands in the block is added to an int64 row in shared memory (exact, so the
+// result equals the staged spread's fixed-point grid bit for bit), then the rows are converted
+// to FP32 and x-transformed in place.  smem: acc rows, twiddles, FFT buffers, candidate lists.
+// ---------------------------------------------------------------------------------------------
+constexpr int kCandCap = 2048;   // candidate atoms staged per round in the spread + x tile
+
+__host__ __device__ inline size_t spread_x_smem_bytes(int nx, int rows) {
+  return (((size_t)rows * nx * 12 + 15) & ~(size_t)15) + sizeof(float2) * ((size_t)nx + 2 * (size_t)nx * (rows + 1)) +
+         sizeof(int) * (32 + 64 + 65 + kCandCap);
+}
+
+// Exact int64 accumulation in shared memory with native 32-bit atomics.  A contribution
+// v = p0 + p1 2^16 + p2 2^32 (p0, p1 in [0, 2^16), p2 = v >> 32 signed) is added to three 32-bit
+// sums without using the atomics' return values (no dependent round trips); each sum stays exact
+// while a point receives fewer than 2^16 contributions, which the tile guarantees by checking
+// its candidate-atom count.  Beyond that the carry form is used: lo (u32) + hi (s32), the wrap of
+// lo detected from the returned old value.
+__device__ __forceinline__ void add_fixed_split3(unsigned int* s0, unsigned int* s1, int* s2, int idx,
+                                                 long long v) {
+  const unsigned long long u = (unsigned long long)v;
+  const unsigned int p0 = (unsigned int)(u & 0xffffull), p1 = (unsigned int)((u >> 16) & 0xffffull);
+  const int p2 = (int)(v >> 32);
+  atomicAdd(&s0[idx], p0);
+  atomicAdd(&s1[idx], p1);
+  if (p2 != 0) atomicAdd(&s2[idx], p2);
+}
+
+__device__ __forceinline__ void add_fixed_carry(unsigned int* lo, int* hi, int idx, long long v) {
+  const unsigned int l = (unsigned int)(unsigned long long)v;
+  const int h = (int)(v >> 32);
+  const unsigned int old = atomicAdd(&lo[idx], l);
+  const int carry = (old + l) < old ? 1 : 0;
+  if (h + carry != 0) atomicAdd(&hi[idx], h + carry);
+}
+
+template <int P, bool SPLIT3>
+__device__ __forceinline__ void spread_atom_rows(const SysDesc& d, int i, int Y0, int Z0, int nry,
+                                                 int nrz, unsigned int* s0, unsigned int* s1, int* s2) {
+  const Geom& g = d.g;
+  const float4 a = __ldg(&d.xyzq[i]);
+  int ix, iy, iz;
+  float ux, uy, uz, tx[P], ty[P], tz[P];
+  frac_coord(a.y, g.sy_hi, g.sy_lo, g.ny, iy, uy);
+  frac_coord(a.z, g.sz_hi, g.sz_lo, g.nz, iz, uz);
+  // rows of this atom inside the block (relative), -1 if outside
+  int ry[P], rz[P];
+  bool any_y = false, any_z = false;
+#pragma unroll
+  for (int b = 0; b < P; b++) {
+    int y = wrap_add(iy, b, g.ny) - Y0;
+    if (y < 0) y += g.ny;
+    ry[b] = y < nry ? y : -1;
+    any_y |= y < nry;
+    int z = wrap_add(iz, b, g.nz) - Z0;
+    if (z < 0) z += g.nz;
+    rz[b] = z < nrz ? z : -1;
+    any_z |= z < nrz;
+  }
+  if (!(any_y && any_z)) return;
+  frac_coord(a.x, g.sx_hi, g.sx_lo, g.nx, ix, ux);
+  bspline<P>(ux, tx, nullptr);
+#pragma unroll
+  for (int k = 0; k < P; k++) tx[k] = __fmul_rn(a.w, tx[k]);
+  bspline<P>(uy, ty, nullptr);
+  bspline<P>(uz, tz, nullptr);
+  int xs[P];
+#pragma unroll
+  for (int k = 0; k < P; k++) xs[k] = wrap_add(ix, k, g.nx);
+  const int nx = g.nx;
+#pragma unroll
+  for (int c = 0; c < P; c++) {
+    if (rz[c] < 0) continue;
+#pragma unroll
+    for (int b = 0; b < P; b++) {
+      if (ry[b] < 0) continue;
+      const int row = (ry[b] + nry * rz[c]) * nx;
+#pragma unroll
+      for (int k = 0; k < P; k++) {
+        const long long v = fixed_contrib(tx[k], ty[b], tz[c]);
+        if (SPLIT3) add_fixed_split3(s0, s1, s2, row + xs[k], v);
+        else add_fixed_carry(s0, s2, row + xs[k], v);
+      }
+    }
+  }
+}
+
+template <int P>
+__device__ __forceinline__ void spread_x_tile(const SysDesc& d, int tile, int parity, char* smem_raw) {
+  const Geom& g = d.g;
+  const FftPlan1D& plan = d.px;
+  const int L = g.nx;
+  const int by = tile % d.nby, bz = tile / d.nby;
+  const int Y0 = by * d.bry, Z0 = bz * d.brz;
+  const int nry = min(d.bry, g.ny - Y0), nrz = min(d.brz, g.nz - Z0);
+  const int rows = d.bry * d.brz;            // FFT lines of the tile (rows beyond nry*nrz are 0)
+  const int ld = rows + 1;
+  unsigned int* s0 = (unsigned int*)smem_raw;
+  unsigned int* s1 = s0 + (size_t)rows * L;
+  int* s2 = (int*)(s1 + (size_t)rows * L);
+  float2* tw = (float2*)(smem_raw + (((size_t)rows * L * 12 + 15) & ~(size_t)15));
+  float2* b0 = tw + L;
+  float2* b1 = b0 + (size_t)L * ld;
+  int* cand = (int*)(b1 + (size_t)L * ld);   // [0..7] y bins, [8..15] z bins, [16] #y, [17] #z
+  const int tid = threadIdx.x;
+  const int nbins = d.nby * d.nbz;
+  step_mark(d, 0);
+  for (int idx = tid; idx < rows * L; idx += kThreads) {
+    s0[idx] = 0u;
+    s1[idx] = 0u;
+    s2[idx] = 0;
+  }
+  for (int i = tid; i < L; i += kThreads) tw[i] = __ldg(&d.tw[plan.tw_off + i]);
+  // Candidate bins: the origin rows Y0-P+1 .. Y0+nry-1 (wrapped) cover consecutive bins
+  // b0, b0+1, ..., by (mod nby); all bins when the window spans the whole axis.  Same for z.
+  // At most ceil((P-1)/bry) + 2 <= 8 bins per axis.
+  if (tid < 2) {
+    const int n = tid == 0 ? g.ny : g.nz, br = tid == 0 ? d.bry : d.brz;
+    const int nb = tid == 0 ? d.nby : d.nbz, own = tid == 0 ? by : bz;
+    const int R0 = tid == 0 ? Y0 : Z0, nr = tid == 0 ? nry : nrz;
+    const int W = P - 1 + nr;
+    int* out = cand + 8 * tid;
+    if (W >= n) {
+      for (int k = 0; k < nb; k++) out[k] = k;
+      cand[16 + tid] = nb;
+    } else {
+      int r0 = (R0 - P + 1) % n;
+      if (r0 < 0) r0 += n;
+      const int b0 = r0 / br;
+      int cnt = own - b0;
+      if (cnt < 0) cnt += nb;
+      cnt += 1;
+      for (int k = 0; k < cnt; k++) {
+        const int b = b0 + k;
+        out[k] = b >= nb ? b - nb : b;
+      }
+      cand[16 + tid] = cnt;
+    }
+  }
+  __syncthreads();
+  // candidate atoms: counts of all candidate bins in parallel, then their atom lists into smem
+  const int ncy = cand[16], ncz = cand[17], nc = ncy * ncz;
+  int* ccnt = cand + 32;                       // [64] counts, [65..129] offsets
+  int* coff = ccnt + 64;
+  int* clist = coff + 65;                      // [kCandCap] atom indices
+  if (tid < nc) {
+    const int b = cand[tid % ncy] + d.nby * cand[8 + tid / ncy];
+    ccnt[tid] = min(__ldcg(&d.bin_count[parity * nbins + b]), d.bin_cap);
+  }
+  __syncthreads();
+  if (tid == 0) {
+    int o = 0;
+    for (int c = 0; c < nc; c++) { coff[c] = o; o += ccnt[c]; }
+    coff[nc] = o;
+  }
+  __syncthreads();
+  const int total = coff[nc];
+  step_mark(d, 1);
+  const int novf = __ldcg(&d.ovf_count[parity]);
+  // fewer than 2^16 candidates => fewer than 2^16 contributions per point: the split form is exact
+  const bool split3 = total + novf < 65536;
+  for (int base0 = 0; base0 < total + novf; base0 += kCandCap) {
+    const int m = min(kCandCap, total + novf - base0);
+    for (int j = tid; j < m; j += kThreads) {
+      const int q = base0 + j;
+      int atom;
+      if (q < total) {
+        int c = 0;
+        while (q >= coff[c + 1]) c++;
+        const int b = cand[c % ncy] + d.nby * cand[8 + c / ncy];
+        atom = __ldcg(&d.bin_atoms[(size_t)b * d.bin_cap + (q - coff[c])]);
+      } else {
+        atom = __ldcg(&d.ovf_atoms[q - total]);
+      }
+      clist[j] = atom;
+    }
+    __syncthreads();
+    step_mark(d, 2);
+    if (split3)
+      for (int j = tid; j < m; j += kThreads) spread_atom_rows<P, true>(d, clist[j], Y0, Z0, nry, nrz, s0, s1, s2);
+    else
+      for (int j = tid; j < m; j += kThreads) spread_atom_rows<P, false>(d, clist[j], Y0, Z0, nry, nrz, s0, s1, s2);
+    __syncthreads();
+    step_mark(d, 3);
+  }
+  // the other parity's counters are cleared for the next launch by the system's first block
+  if (tile == 0) {
+    for (int j = tid; j < nbins; j += kThreads) d.bin_count[(1 - parity) * nbins + j] = 0;
+    if (tid == 0) d.ovf_count[1 - parity] = 0;
+  }
+  __syncthreads();
+  // rows: r = ry + nry*rz (r < nry*nrz valid); FFT line t = r
+  for (int idx = tid; idx < rows * L; idx += kThreads) {
+    const int t = fdiv(idx, plan.n_div), e = idx - t * L;
+    // split: p0 + p1 2^16 + p2 2^32; carry form: s0 = lo, s1 = 0, s2 = hi -- one formula
+    const unsigned long long u = (unsigned long long)s0[idx] + ((unsigned long long)s1[idx] << 16) +
+                                 ((unsigned long long)(unsigned int)s2[idx] << 32);
+    b0[e * ld + t] = make_float2(fixed_to_float((long long)u), 0.0f);
+  }
+  __syncthreads();
+  step_mark(d, 4);
+  TileLane ln(tid, kThreads, rows);
+  float2* res = fft_tile(b0, b1, plan, ld, 1, ln, tw, false);
+  step_mark(d, 5);
+  const int hx = g.hx;
+  const FastDiv rd = make_fastdiv(rows), nryd = make_fastdiv(nry);
+  const int nvalid = nry * nrz;
+  for (int idx = tid; idx < hx * rows; idx += kThreads) {
+    const int k = fdiv(idx, rd), t = idx - k * rows;
+    if (t < nvalid) {
+      const int rz = fdiv(t, nryd), ry = t - rz * nry;
+      __stcg(&d.cgrid[cidx(g, k, Z0 + rz, Y0 + ry)], res[k * ld + t]);
+    }
+  }
+  __syncthreads();
+  step_mark(d, 6);
+}
+
+__device__ __forceinline__ void spread_x_dispatch(const SysDesc& d, int tile, int parity, char* smem) {
+  switch (d.order) {
+    case 4: spread_x_tile<4>(d, tile, parity, smem); break;
+    case 6: spread_x_tile<6>(d, tile, parity, smem); break;
+    default: spread_x_tile<8>(d, tile, parity, smem); break;
+  }
 }
 
 // Convert the accumulators into the FP64 record and clear them (one thread).

@@ -250,6 +250,10 @@ class CudaPMERecip:
         C.check(self._lib.pme_get_status(self._h, ctypes.byref(st)), "get_status")
         return st.value
 
+    def reserve_atoms(self, natom: int):
+        """Pre-size the fused evaluation's atom bins (call before CUDA-graph capture)."""
+        C.check(self._lib.pme_reserve_atoms(self._h, int(natom)), "reserve_atoms")
+
     def set_barrier_spin_limit(self, polls: int):
         C.check(self._lib.pme_set_barrier_spin_limit(self._h, int(polls)), "set_barrier_spin_limit")
 
@@ -260,6 +264,10 @@ class CudaPMERecip:
             C.check(self._lib.pme_set_trace(self._h, None, 0), "set_trace")
         else:
             C.check(self._lib.pme_set_trace(self._h, _ptr(buf), int(max_ctas or buf.numel() // 14)), "set_trace")
+
+    def set_fft_schedule(self, schedule: int):
+        """PME_SCHED_AUTO / PME_SCHED_PLANES / PME_SCHED_PASSES (identical results)."""
+        C.check(self._lib.pme_set_fft_schedule(self._h, int(schedule)), "set_fft_schedule")
 
     def set_fault_injection(self, what: int):
         C.check(self._lib.pme_set_fault_injection(self._h, int(what)), "set_fault_injection")

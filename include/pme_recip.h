@@ -119,6 +119,17 @@ PME_API int pme_load_charge_grid(pme_recip* h, const float* host_in);
  * together with the barrier words and the accumulation grid, so the handle is usable again. */
 PME_API int pme_get_status(pme_recip* h, int* device_status);
 PME_API int pme_set_barrier_spin_limit(pme_recip* h, unsigned int polls);   /* default 2^22 */
+/* The fused evaluation bins atoms by grid row block; its bin storage grows (synchronously) the
+ * first time a call has more atoms than any earlier one.  Call this with the largest atom count
+ * before capturing evaluations in a CUDA graph, so that no capture needs to allocate. */
+PME_API int pme_reserve_atoms(pme_recip* h, int natom);
+/* Schedule of the fused evaluation's y/z transforms: PME_SCHED_PLANES runs y, z and the solve
+ * as whole-plane tiles (one CTA per kx plane, where a plane fits in shared memory),
+ * PME_SCHED_PASSES as separate y and z passes (more, smaller tiles), PME_SCHED_AUTO (default)
+ * picks planes only when there are at least as many planes as SMs.  Results are identical. */
+enum { PME_SCHED_AUTO = 0, PME_SCHED_PLANES = 1, PME_SCHED_PASSES = 2 };
+PME_API int pme_set_fft_schedule(pme_recip* h, int schedule);
+
 /* Test hook for failure detection: PME_INJECT_SKIP_BARRIER makes CTA 0 of the next fused
  * evaluations leave before the first grid barrier, so the other CTAs' bounded waits run out
  * (no fault, no hang).  PME_INJECT_NONE turns it off. */
@@ -128,7 +139,8 @@ PME_API int pme_set_fault_injection(pme_recip* h, int what);
 /* Profiling hook: while set, every fused evaluation writes, for each CTA c < max_ctas and each of
  * its 7 phases p (spread, x fwd, y fwd, z fwd+solve+inv, y inv, x inv, gather), the %globaltimer
  * (ns) at the phase's start and end to dev_buf[(c * 7 + p) * 2 + {0, 1}] (device memory,
- * max_ctas * 14 entries).  NULL turns it off. */
+ * max_ctas * 14 entries), followed by 32 entries of step stamps inside CTA 0's first tiles.
+ * NULL turns it off. */
 PME_API int pme_set_trace(pme_recip* h, unsigned long long* dev_buf, int max_ctas);
 
 /* ---- batches: many independent systems in one persistent launch ----

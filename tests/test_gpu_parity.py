@@ -36,6 +36,9 @@ def _sys(name):
     if name == "one_atom":
         return S.PmeSystem("one", np.array([[1.3, 2.7, 4.1, 0.5]], np.float32), (10.0, 10.0, 10.0),
                            (16, 16, 16), 4, 0.4)
+    if name == "long_z":      # nz > 256: the fused path runs separate y / z passes, not plane tiles
+        box = (15.0, 16.0, 300.0)
+        return S.PmeSystem("lz", S.water_box(1500, box, 34), box, (16, 18, 320), 4, 0.35)
     if name == "ragged33":
         box = (15.0, 15.0, 15.0)
         x = S.water_box(11, box, 33)
@@ -44,7 +47,7 @@ def _sys(name):
 
 
 CASES = ["water1k_32", "water8k_64_p4", "water8k_64_p6", "water1k_p8", "odd_grid", "noncubic_p6",
-         "one_atom", "ragged33"]
+         "one_atom", "ragged33", "long_z"]
 
 
 def _pme(cuda, s):
@@ -136,12 +139,17 @@ def test_reference_fixture(cuda, ref_fixture, order):
     assert np.abs(got["force"] - f[f"force{order}"]).max() < f[f"tol_force{order}"]
 
 
-def test_staged_calls_equal_fused_eval(cuda):
-    s = _sys("water8k_64_p4")
+@pytest.mark.parametrize("name,schedule", [("water8k_64_p4", 1), ("water8k_64_p4", 2),
+                                           ("long_z", 0), ("noncubic_p6", 1)])
+def test_staged_calls_equal_fused_eval(cuda, name, schedule):
+    """Staged reference-style calls and the fused kernel (either y/z schedule) agree bit for bit."""
+    s = _sys(name)
     a = _run(cuda, s, staged=True)
-    b = _run(cuda, s, staged=False)
+    pme = _pme(cuda, s)
+    pme.set_fft_schedule(schedule)
+    b = _run(cuda, s, staged=False, pme=pme)
     assert np.array_equal(a["force"], b["force"])
-    assert a["energy"] == b["energy"]
+    assert a["energy"] == b["energy"] and a["energy_self"] == b["energy_self"]
     assert np.array_equal(a["virial"], b["virial"])
 
 
