@@ -69,6 +69,7 @@ SIGNATURES = {
     "pme_batch_info": [_P, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(ctypes.c_size_t)],
     "pme_system_device_bytes": [_I, _I, _I],
     "pme_set_trace": [_P, _P, _I],
+    "pme_spread_charge_noalloc": [_P, _I, _DP, _I, _I, _I, _I, _P, _P],
     "pme_batch_set_trace": [_P, _P, _I],
     "pme_last_error_string": [],
     "pme_status_string": [_I],

@@ -314,6 +314,10 @@ struct SystemState {
 
 }  // namespace
 
+namespace pme {
+void set_last_error(const char* msg) { g_err = msg ? msg : ""; }
+}  // namespace pme
+
 struct pme_recip {
   int fft_type = PME_FFT_BOX;
   int* d_bins = nullptr;

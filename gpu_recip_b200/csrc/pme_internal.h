@@ -35,6 +35,9 @@ struct FusedArgs {
 
 cudaError_t configure_kernels(size_t* max_dyn_smem);
 
+// Record the calling thread's last error message (returned by pme_last_error_string).
+void set_last_error(const char* msg);
+
 size_t spread_smem(int order);
 size_t fused_smem_bytes(const SysDesc& d);
 void fused_tile_counts(const SysDesc& d, int* counts);

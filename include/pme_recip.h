@@ -177,6 +177,21 @@ PME_API int pme_batch_set_trace(pme_batch* b, unsigned long long* dev_buf, int m
 /* Device bytes one system of this grid occupies (for admission by HBM footprint). */
 PME_API size_t pme_system_device_bytes(int nfftx, int nffty, int nfftz);
 
+/* ---- spreading without device allocation ----
+ * No counterpart in the reference.  For callers that must not allocate device memory when they
+ * need a charge grid: code running while a stream is captured into a CUDA graph, hosts whose own
+ * memory manager owns all device memory, and latency-critical loops that cannot take allocator
+ * locks.  Same spreading kernel and exact int64 fixed-point accumulation as pme_spread_charge,
+ * but the accumulation grid is a fixed array compiled into this library (8 MiB on every GPU that
+ * loads it, so nfftx*nffty*nfftz <= 1048576; larger grids return PME_EINVAL).  The caller passes
+ * the coordinates (device float4[ncoord]), the host recip[9] and the output: grid_out, a device
+ * float[nfftz][nffty][nfftx] that receives the converted charge grid.  Asynchronous on `stream`.
+ * The first call on a device looks up the array's device address (cudaGetSymbolAddress): make it
+ * before any stream capture.  All calls share the array and each clears it before use: calls
+ * whose work overlaps on the GPU race and corrupt each other's grid. */
+PME_API int pme_spread_charge_noalloc(const void* xyzq, int ncoord, const double* recip, int nfftx,
+                                      int nffty, int nfftz, int order, float* grid_out, void* stream);
+
 /* ---- errors / version ---- */
 PME_API const char* pme_last_error_string(void);     /* thread-local message of the last failure */
 PME_API const char* pme_status_string(int status);
