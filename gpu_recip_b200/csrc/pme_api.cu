@@ -168,7 +168,7 @@ struct SystemState {
   int tx_rows = 0, tx_y = 0, tx_z = 0, plane = 0;
   int bry = 4, brz = 4, nby = 1, nbz = 1;
   int bin_cap = 0, atom_cap = 0;
-  int* bins = nullptr;       // [2 nbins counts][nbins*bin_cap atoms][2 ovf counts][atom_cap ovf]
+  int* bins = nullptr;       // [2 nbins counts][nbins*bin_cap records][2 ovf counts][atom_cap ovf records]
   unsigned long long* accum = nullptr;
   float2* cgrid = nullptr;
   float* rgrid = nullptr;
@@ -202,9 +202,9 @@ struct SystemState {
     // whole-plane tiles need one thread per line of each orientation and the plane in smem
     plane = (plane_smem_bytes(ny, nz) <= kTileSmemBudget && ny <= kThreads && nz <= kThreads) ? 1 : 0;
     // row blocks of the fused spread + x pass: the largest square block that fits
-    for (int b = 4; b >= 1; b--) {
+    for (int b = kSpreadMaxBlock; b >= 1; b--) {
       bry = brz = b;
-      if (spread_x_smem_bytes(nx, b * b) <= kTileSmemBudget) break;
+      if (spread_x_smem_bytes(nx, b * b, kMaxOrder) <= kTileSmemBudget) break;
     }
     nby = (ny + bry - 1) / bry;
     nbz = (nz + brz - 1) / brz;
@@ -214,8 +214,12 @@ struct SystemState {
 
   // bin storage for up to natom atoms: capacity 1.5x the mean occupancy + 32 per bin
   static int cap_for(int natom, int nbins) { return std::max(32, (int)(1.5 * natom / nbins) + 32); }
+  // counts (padded to 16 bytes), bin records, overflow counts (padded), overflow records; records
+  // are sized for order 8
+  size_t count_ints() const { return (2 * (size_t)nbins() + 3) & ~(size_t)3; }
   size_t bin_ints(int natom) const {
-    return 2 * (size_t)nbins() + (size_t)nbins() * cap_for(natom, nbins()) + 2 + (size_t)std::max(natom, 1);
+    return count_ints() + (size_t)nbins() * cap_for(natom, nbins()) * rec_floats(kMaxOrder) + 4 +
+           (size_t)std::max(natom, 1) * rec_floats(kMaxOrder);
   }
 
   void carve(char* base) {
@@ -304,9 +308,9 @@ struct SystemState {
     if (bins) {
       const size_t nb = nbins();
       d.bin_count = bins;
-      d.bin_atoms = bins + 2 * nb;
-      d.ovf_count = bins + 2 * nb + nb * (size_t)bin_cap;
-      d.ovf_atoms = d.ovf_count + 2;
+      d.bin_recs = (float*)(bins + count_ints());
+      d.ovf_count = (int*)(d.bin_recs + nb * (size_t)bin_cap * rec_floats(kMaxOrder));
+      d.ovf_recs = (float*)(d.ovf_count + 4);
     }
     return d;
   }

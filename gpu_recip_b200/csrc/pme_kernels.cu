@@ -218,7 +218,7 @@ __global__ void __launch_bounds__(kThreads) k_fused(FusedArgs a) {
           if (local < tiles_xpass(d)) x_inv_tile(d, local, smem);
           else if (threadIdx.x == 0) finalize_system(d, true, true);
           break;
-        default: gather_dispatch(d, local); break;
+        default: gather_bin_dispatch(d, local, parity); break;
       }
       __syncthreads();
     }
@@ -250,7 +250,7 @@ size_t fused_smem_bytes(const SysDesc& d) {
   size_t m = 32 * sizeof(long long);
   size_t c[5] = {staged_fft_smem(d.g.nx, d.tx_rows), staged_fft_smem(d.g.ny, d.tx_y),
                  staged_z_smem(d), d.plane ? plane_smem_bytes(d.g.ny, d.g.nz) : 0,
-                 spread_x_smem_bytes(d.g.nx, d.bry * d.brz)};
+                 spread_x_smem_bytes(d.g.nx, d.bry * d.brz, d.order)};
   for (size_t v : c) m = m > v ? m : v;
   return m;
 }
@@ -262,7 +262,7 @@ void fused_tile_counts(const SysDesc& d, int* counts) {
   counts[3] = d.plane ? 0 : tiles_zpass(d);
   counts[4] = d.plane ? 0 : tiles_ypass(d);
   counts[5] = tiles_xpass(d) + 1;
-  counts[6] = tiles_gather(d);
+  counts[6] = tiles_blocks(d);
 }
 
 int fused_barriers(const int* total) {

@@ -62,9 +62,9 @@ struct SysDesc {
   int bry, brz, nby, nbz;
   int bin_cap;
   int* bin_count;            // [2][nby*nbz]
-  int* bin_atoms;            // [nby*nbz][bin_cap]
+  float* bin_recs;           // [nby*nbz][bin_cap] atom records of rec_floats(order) floats
   int* ovf_count;            // [2]
-  int* ovf_atoms;            // [natom capacity]
+  float* ovf_recs;           // [natom capacity] records of the atoms beyond a bin's capacity
   unsigned long long* steps; // profiling: %globaltimer at the steps of CTA 0's tiles (or null)
 };
 
@@ -557,26 +557,48 @@ __device__ __forceinline__ void plane_tile(const SysDesc& d, int kx, float2* sme
 
 // ---------------------------------------------------------------------------------------------
 // Fused path, phase 0: bin kThreads atoms by the row block of their stencil origin; sum q^2.
+// A bin entry is the atom's record: stencil origin (ix, iy, iz as int bits) and atom index, then
+// the FP32 spreading weights q*thx[P], thy[P], thz[P] -- the values the staged spread uses --
+// padded to a multiple of 4 floats so that every record is 16-byte aligned.
 // ---------------------------------------------------------------------------------------------
-__device__ __forceinline__ void bin_tile(const SysDesc& d, int tile, int parity, long long* red) {
+__host__ __device__ constexpr int rec_floats(int order) { return (4 + 3 * order + 3) & ~3; }
+
+template <int P>
+__device__ __forceinline__ void bin_tile_p(const SysDesc& d, int tile, int parity, long long* red) {
+  constexpr int RF = rec_floats(P);
   const Geom& g = d.g;
   const int i = tile * kThreads + threadIdx.x;
   const int nbins = d.nby * d.nbz;
   long long q2 = 0;
   if (i < d.natom) {
     const float4 a = __ldg(&d.xyzq[i]);
-    int iy, iz;
-    float u;
-    frac_coord(a.y, g.sy_hi, g.sy_lo, g.ny, iy, u);
-    frac_coord(a.z, g.sz_hi, g.sz_lo, g.nz, iz, u);
+    int ix, iy, iz;
+    float ux, uy, uz;
+    frac_coord(a.x, g.sx_hi, g.sx_lo, g.nx, ix, ux);
+    frac_coord(a.y, g.sy_hi, g.sy_lo, g.ny, iy, uy);
+    frac_coord(a.z, g.sz_hi, g.sz_lo, g.nz, iz, uz);
+    float w[RF - 4];
+#pragma unroll
+    for (int k = 3 * P; k < RF - 4; k++) w[k] = 0.0f;
+    bspline<P>(ux, w, nullptr);
+#pragma unroll
+    for (int k = 0; k < P; k++) w[k] = __fmul_rn(a.w, w[k]);
+    bspline<P>(uy, w + P, nullptr);
+    bspline<P>(uz, w + 2 * P, nullptr);
     const int b = iy / d.bry + d.nby * (iz / d.brz);
     const int slot = atomicAdd(&d.bin_count[parity * nbins + b], 1);
+    float* rec;
     if (slot < d.bin_cap) {
-      d.bin_atoms[(size_t)b * d.bin_cap + slot] = i;
+      rec = d.bin_recs + ((size_t)b * d.bin_cap + slot) * RF;
     } else {
       const int o = atomicAdd(&d.ovf_count[parity], 1);
-      d.ovf_atoms[o] = i;
+      rec = d.ovf_recs + (size_t)o * RF;
     }
+    float4* r4 = (float4*)rec;
+    __stcg(&r4[0], make_float4(__int_as_float(ix), __int_as_float(iy), __int_as_float(iz), __int_as_float(i)));
+#pragma unroll
+    for (int c = 0; c < (RF - 4) / 4; c++)
+      __stcg(&r4[1 + c], make_float4(w[4 * c], w[4 * c + 1], w[4 * c + 2], w[4 * c + 3]));
     q2 = q2_fixed(a.w);
   }
   if (d.calc_self) {
@@ -586,27 +608,53 @@ __device__ __forceinline__ void bin_tile(const SysDesc& d, int tile, int parity,
   __syncthreads();
 }
 
+__device__ __forceinline__ void bin_tile(const SysDesc& d, int tile, int parity, long long* red) {
+  switch (d.order) {
+    case 4: bin_tile_p<4>(d, tile, parity, red); break;
+    case 6: bin_tile_p<6>(d, tile, parity, red); break;
+    default: bin_tile_p<8>(d, tile, parity, red); break;
+  }
+}
+
 // ---------------------------------------------------------------------------------------------
 // Fused path, phase 1: spread + x forward for one row block (rows y in [Y0, Y0+bry), z in
-// [Z0, Z0+brz), all x).  The block's candidate atoms are those binned in the row blocks whose
-// origins can reach it (origin rows Y0-P+1 .. Y0+bry-1, wrapped), plus the overflow list.  Each
-// contribution that lands in the block is added to an int64 row in shared memory (exact, so the
-// result equals the staged spread's fixed-point grid bit for bit), then the rows are converted
-// to FP32 and x-transformed in place.  smem: acc rows, twiddles, FFT buffers, candidate lists.
+// [Z0, Z0+brz), all x).  The block's candidate atoms are the records of the row blocks whose
+// origins can reach it (origin rows Y0-P+1 .. Y0+bry-1, wrapped), plus the overflow records.
+// Each contribution that lands in the block is added to an int64 row in shared memory (exact, so
+// the result equals the staged spread's fixed-point grid bit for bit), then the rows are converted
+// to FP32 and x-transformed in place.
+//
+// The work is split so that every lane does the same amount: a round takes up to kSpreadSlots
+// candidates; step A tests each against the block and lists the ones that reach it (their x
+// weights and their y/z weights re-indexed by block row) and one item per (atom, block row) it
+// covers; step B gives each lane one item at a time, i.e. the P contributions of one stencil row.
+// The accumulator rows have an odd stride, so the rows of one atom fall in different banks.
 // ---------------------------------------------------------------------------------------------
-constexpr int kCandCap = 2048;   // candidate atoms staged per round in the spread + x tile
+constexpr int kSpreadSlots = 2 * kThreads;          // candidates per round (listed-atom slots)
+constexpr int kSpreadMaxBlock = 4;                  // row-block edge limit (bry, brz)
+constexpr int kSpreadItemCap = kSpreadSlots * kSpreadMaxBlock * kSpreadMaxBlock;
+constexpr int kSpreadBookInts = 168;                // candidate bins, counts, offsets, counters
 
-__host__ __device__ inline size_t spread_x_smem_bytes(int nx, int rows) {
-  return (((size_t)rows * nx * 12 + 15) & ~(size_t)15) + sizeof(float2) * ((size_t)nx + 2 * (size_t)nx * (rows + 1)) +
-         sizeof(int) * (32 + 64 + 65 + kCandCap);
+__host__ __device__ inline int spread_row_stride(int nx) { return nx | 1; }
+__host__ __device__ inline size_t align16(size_t b) { return (b + 15) & ~(size_t)15; }
+
+// smem of the spread + x tile: 3 x 32-bit accumulators per point, twiddles, bookkeeping, then a
+// work area that holds the listed atoms and items while spreading and the FFT buffers after.
+__host__ __device__ inline size_t spread_x_smem_bytes(int nx, int rows, int order) {
+  const size_t acc = align16((size_t)rows * spread_row_stride(nx) * 12);
+  const size_t fft = (size_t)2 * nx * (rows + 1) * sizeof(float2);
+  const size_t lists = (size_t)kSpreadSlots * (1 + order + 2 * kSpreadMaxBlock) * 4 +
+                       (size_t)kSpreadItemCap * sizeof(unsigned short);
+  return acc + align16((size_t)nx * sizeof(float2)) + kSpreadBookInts * sizeof(int) + (fft > lists ? fft : lists);
 }
 
 // Exact int64 accumulation in shared memory with native 32-bit atomics.  A contribution
 // v = p0 + p1 2^16 + p2 2^32 (p0, p1 in [0, 2^16), p2 = v >> 32 signed) is added to three 32-bit
-// sums without using the atomics' return values (no dependent round trips); each sum stays exact
-// while a point receives fewer than 2^16 contributions, which the tile guarantees by checking
-// its candidate-atom count.  Beyond that the carry form is used: lo (u32) + hi (s32), the wrap of
-// lo detected from the returned old value.
+// sums without using the atomics' return values (no dependent round trips).  The p0 and p1 sums
+// cannot wrap while a point receives at most 2^16 contributions, which the tile guarantees by
+// checking its candidate count; the p2 sum may wrap, harmlessly, since only its value modulo 2^32
+// enters the int64 result.  Beyond that count the carry form is used: lo (u32) + hi (s32), the
+// wrap of lo detected from the returned old value.
 __device__ __forceinline__ void add_fixed_split3(unsigned int* s0, unsigned int* s1, int* s2, int idx,
                                                  long long v) {
   const unsigned long long u = (unsigned long long)v;
@@ -625,78 +673,156 @@ __device__ __forceinline__ void add_fixed_carry(unsigned int* lo, int* hi, int i
   if (h + carry != 0) atomicAdd(&hi[idx], h + carry);
 }
 
-template <int P, bool SPLIT3>
-__device__ __forceinline__ void spread_atom_rows(const SysDesc& d, int i, int Y0, int Z0, int nry,
-                                                 int nrz, unsigned int* s0, unsigned int* s1, int* s2) {
+// The listed atoms of a round, structure of arrays over kSpreadSlots slots:
+//   ix[slot]; w[k][slot] = q thx[k] (k < P); w[P + ry][slot] = thy of block row ry;
+//   w[P + kSpreadMaxBlock + rz][slot] = thz of block row rz.
+// An item is slot | ry << 9 | rz << 11.
+struct SpreadLists {
+  int* ix;
+  float* w;
+  unsigned short* items;
+  int* counters;   // [0] listed atoms, [1] items
+};
+
+// Step A for one candidate record per lane (rec == nullptr: no candidate).  Every lane of the
+// warp calls it.
+template <int P>
+__device__ __forceinline__ void spread_list_atom(const SysDesc& d, const float* rec, int Y0, int Z0, int nry,
+                                                 int nrz, const SpreadLists& sl) {
+  constexpr int S = kSpreadSlots;
   const Geom& g = d.g;
-  const float4 a = __ldg(&d.xyzq[i]);
-  int ix, iy, iz;
-  float ux, uy, uz, tx[P], ty[P], tz[P];
-  frac_coord(a.y, g.sy_hi, g.sy_lo, g.ny, iy, uy);
-  frac_coord(a.z, g.sz_hi, g.sz_lo, g.nz, iz, uz);
-  // rows of this atom inside the block (relative), -1 if outside
-  int ry[P], rz[P];
-  bool any_y = false, any_z = false;
-#pragma unroll
-  for (int b = 0; b < P; b++) {
-    int y = wrap_add(iy, b, g.ny) - Y0;
-    if (y < 0) y += g.ny;
-    ry[b] = y < nry ? y : -1;
-    any_y |= y < nry;
-    int z = wrap_add(iz, b, g.nz) - Z0;
-    if (z < 0) z += g.nz;
-    rz[b] = z < nrz ? z : -1;
-    any_z |= z < nrz;
-  }
-  if (!(any_y && any_z)) return;
-  frac_coord(a.x, g.sx_hi, g.sx_lo, g.nx, ix, ux);
-  bspline<P>(ux, tx, nullptr);
-#pragma unroll
-  for (int k = 0; k < P; k++) tx[k] = __fmul_rn(a.w, tx[k]);
-  bspline<P>(uy, ty, nullptr);
-  bspline<P>(uz, tz, nullptr);
-  int xs[P];
-#pragma unroll
-  for (int k = 0; k < P; k++) xs[k] = wrap_add(ix, k, g.nx);
-  const int nx = g.nx;
-#pragma unroll
-  for (int c = 0; c < P; c++) {
-    if (rz[c] < 0) continue;
+  const int lane = threadIdx.x & 31;
+  unsigned int my = 0u, mz = 0u;   // block rows covered by the stencil
+  int ix = 0, ry0 = 0, rz0 = 0;
+  if (rec != nullptr) {
+    const float4 h = __ldcg((const float4*)rec);
+    ix = __float_as_int(h.x);
+    ry0 = __float_as_int(h.y) - Y0;
+    if (ry0 < 0) ry0 += g.ny;
+    rz0 = __float_as_int(h.z) - Z0;
+    if (rz0 < 0) rz0 += g.nz;
 #pragma unroll
     for (int b = 0; b < P; b++) {
-      if (ry[b] < 0) continue;
-      const int row = (ry[b] + nry * rz[c]) * nx;
+      int y = ry0 + b;
+      if (y >= g.ny) y -= g.ny;
+      if (y < nry) my |= 1u << y;
+      int z = rz0 + b;
+      if (z >= g.nz) z -= g.nz;
+      if (z < nrz) mz |= 1u << z;
+    }
+  }
+  const int nrow = __popc(my) * __popc(mz);
+  const unsigned int act = __ballot_sync(0xffffffffu, nrow > 0);
+  if (act == 0u) return;
+  int incl = nrow;
 #pragma unroll
-      for (int k = 0; k < P; k++) {
-        const long long v = fixed_contrib(tx[k], ty[b], tz[c]);
-        if (SPLIT3) add_fixed_split3(s0, s1, s2, row + xs[k], v);
-        else add_fixed_carry(s0, s2, row + xs[k], v);
-      }
+  for (int o = 1; o < 32; o <<= 1) {
+    const int t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
+  }
+  const int wtot = __shfl_sync(0xffffffffu, incl, 31);
+  int sbase = 0, ibase = 0;
+  if (lane == 0) {
+    sbase = atomicAdd(&sl.counters[0], __popc(act));
+    ibase = atomicAdd(&sl.counters[1], wtot);
+  }
+  sbase = __shfl_sync(0xffffffffu, sbase, 0);
+  ibase = __shfl_sync(0xffffffffu, ibase, 0);
+  if (nrow == 0) return;
+  const int slot = sbase + __popc(act & ((1u << lane) - 1u));
+  constexpr int NW = rec_floats(P) - 4;
+  float w[NW];
+  const float4* r4 = (const float4*)rec + 1;
+#pragma unroll
+  for (int c = 0; c < NW / 4; c++) {
+    const float4 v = __ldcg(&r4[c]);
+    w[4 * c] = v.x;
+    w[4 * c + 1] = v.y;
+    w[4 * c + 2] = v.z;
+    w[4 * c + 3] = v.w;
+  }
+  sl.ix[slot] = ix;
+#pragma unroll
+  for (int k = 0; k < P; k++) sl.w[k * S + slot] = w[k];
+#pragma unroll
+  for (int b = 0; b < P; b++) {
+    int y = ry0 + b;
+    if (y >= g.ny) y -= g.ny;
+    if (y < nry) sl.w[(P + y) * S + slot] = w[P + b];
+    int z = rz0 + b;
+    if (z >= g.nz) z -= g.nz;
+    if (z < nrz) sl.w[(P + kSpreadMaxBlock + z) * S + slot] = w[2 * P + b];
+  }
+  int r = ibase + incl - nrow;
+  unsigned int mzz = mz;
+  while (mzz) {
+    const int rz = __ffs(mzz) - 1;
+    mzz &= mzz - 1;
+    unsigned int myy = my;
+    while (myy) {
+      const int ry = __ffs(myy) - 1;
+      myy &= myy - 1;
+      sl.items[r++] = (unsigned short)(slot | ry << 9 | rz << 11);
+    }
+  }
+}
+
+// Step B: the P contributions of one (atom, block row) item per lane.
+template <int P, bool SPLIT3>
+__device__ __forceinline__ void spread_items(const SpreadLists& sl, int nitems, int nry, int L, int Lp,
+                                             unsigned int* s0, unsigned int* s1, int* s2) {
+  constexpr int S = kSpreadSlots;
+  for (int j = threadIdx.x; j < nitems; j += kThreads) {
+    const unsigned int it = sl.items[j];
+    const int slot = it & 511u, ry = (it >> 9) & 3u, rz = it >> 11;
+    const int ix = sl.ix[slot];
+    const float ty = sl.w[(P + ry) * S + slot];
+    const float tz = sl.w[(P + kSpreadMaxBlock + rz) * S + slot];
+    const int rb = (ry + nry * rz) * Lp;
+#pragma unroll
+    for (int k = 0; k < P; k++) {
+      int x = ix + k;
+      if (x >= L) x -= L;
+      const long long v = fixed_contrib(sl.w[k * S + slot], ty, tz);
+      if (SPLIT3) add_fixed_split3(s0, s1, s2, rb + x, v);
+      else add_fixed_carry(s0, s2, rb + x, v);
     }
   }
 }
 
 template <int P>
 __device__ __forceinline__ void spread_x_tile(const SysDesc& d, int tile, int parity, char* smem_raw) {
+  constexpr int RF = rec_floats(P);
+  constexpr int S = kSpreadSlots;
   const Geom& g = d.g;
   const FftPlan1D& plan = d.px;
-  const int L = g.nx;
+  const int L = g.nx, Lp = spread_row_stride(L);
   const int by = tile % d.nby, bz = tile / d.nby;
   const int Y0 = by * d.bry, Z0 = bz * d.brz;
   const int nry = min(d.bry, g.ny - Y0), nrz = min(d.brz, g.nz - Z0);
   const int rows = d.bry * d.brz;            // FFT lines of the tile (rows beyond nry*nrz are 0)
   const int ld = rows + 1;
-  unsigned int* s0 = (unsigned int*)smem_raw;
-  unsigned int* s1 = s0 + (size_t)rows * L;
-  int* s2 = (int*)(s1 + (size_t)rows * L);
-  float2* tw = (float2*)(smem_raw + (((size_t)rows * L * 12 + 15) & ~(size_t)15));
-  float2* b0 = tw + L;
-  float2* b1 = b0 + (size_t)L * ld;
-  int* cand = (int*)(b1 + (size_t)L * ld);   // [0..7] y bins, [8..15] z bins, [16] #y, [17] #z
   const int tid = threadIdx.x;
+  unsigned int* s0 = (unsigned int*)smem_raw;
+  unsigned int* s1 = s0 + (size_t)rows * Lp;
+  int* s2 = (int*)(s1 + (size_t)rows * Lp);
+  char* p = smem_raw + align16((size_t)rows * Lp * 12);
+  float2* tw = (float2*)p;
+  p += align16((size_t)L * sizeof(float2));
+  int* cand = (int*)p;                         // [0..7] y bins, [8..15] z bins, [16] #y, [17] #z
+  int* ccnt = cand + 32;                       // [64] counts of the candidate bins
+  int* coff = ccnt + 64;                       // [65] their offsets
+  p += kSpreadBookInts * sizeof(int);
+  SpreadLists sl;
+  sl.ix = (int*)p;
+  sl.w = (float*)(sl.ix + S);
+  sl.items = (unsigned short*)(sl.w + (size_t)(P + 2 * kSpreadMaxBlock) * S);
+  sl.counters = cand + 18;
+  float2* b0 = (float2*)p;                     // FFT view of the work area (after spreading)
+  float2* b1 = b0 + (size_t)L * ld;
   const int nbins = d.nby * d.nbz;
   step_mark(d, 0);
-  for (int idx = tid; idx < rows * L; idx += kThreads) {
+  for (int idx = tid; idx < rows * Lp; idx += kThreads) {
     s0[idx] = 0u;
     s1[idx] = 0u;
     s2[idx] = 0;
@@ -727,13 +853,10 @@ __device__ __forceinline__ void spread_x_tile(const SysDesc& d, int tile, int pa
       }
       cand[16 + tid] = cnt;
     }
+    sl.counters[tid] = 0;
   }
   __syncthreads();
-  // candidate atoms: counts of all candidate bins in parallel, then their atom lists into smem
   const int ncy = cand[16], ncz = cand[17], nc = ncy * ncz;
-  int* ccnt = cand + 32;                       // [64] counts, [65..129] offsets
-  int* coff = ccnt + 64;
-  int* clist = coff + 65;                      // [kCandCap] atom indices
   if (tid < nc) {
     const int b = cand[tid % ncy] + d.nby * cand[8 + tid / ncy];
     ccnt[tid] = min(__ldcg(&d.bin_count[parity * nbins + b]), d.bin_cap);
@@ -747,45 +870,46 @@ __device__ __forceinline__ void spread_x_tile(const SysDesc& d, int tile, int pa
   __syncthreads();
   const int total = coff[nc];
   step_mark(d, 1);
-  const int novf = __ldcg(&d.ovf_count[parity]);
-  // fewer than 2^16 candidates => fewer than 2^16 contributions per point: the split form is exact
-  const bool split3 = total + novf < 65536;
-  for (int base0 = 0; base0 < total + novf; base0 += kCandCap) {
-    const int m = min(kCandCap, total + novf - base0);
-    for (int j = tid; j < m; j += kThreads) {
-      const int q = base0 + j;
-      int atom;
+  const int ncand = total + __ldcg(&d.ovf_count[parity]);
+  // at most one contribution per candidate and point: up to 2^16 candidates the split form is exact
+  const bool split3 = ncand <= 65536;
+  for (int base0 = 0; base0 < ncand; base0 += S) {
+#pragma unroll 1
+    for (int h = 0; h < S; h += kThreads) {
+      const int q = base0 + h + tid;
+      const float* rec = nullptr;
       if (q < total) {
         int c = 0;
         while (q >= coff[c + 1]) c++;
         const int b = cand[c % ncy] + d.nby * cand[8 + c / ncy];
-        atom = __ldcg(&d.bin_atoms[(size_t)b * d.bin_cap + (q - coff[c])]);
-      } else {
-        atom = __ldcg(&d.ovf_atoms[q - total]);
+        rec = d.bin_recs + ((size_t)b * d.bin_cap + (q - coff[c])) * RF;
+      } else if (q < ncand) {
+        rec = d.ovf_recs + (size_t)(q - total) * RF;
       }
-      clist[j] = atom;
+      spread_list_atom<P>(d, rec, Y0, Z0, nry, nrz, sl);
     }
     __syncthreads();
-    step_mark(d, 2);
-    if (split3)
-      for (int j = tid; j < m; j += kThreads) spread_atom_rows<P, true>(d, clist[j], Y0, Z0, nry, nrz, s0, s1, s2);
-    else
-      for (int j = tid; j < m; j += kThreads) spread_atom_rows<P, false>(d, clist[j], Y0, Z0, nry, nrz, s0, s1, s2);
+    if (base0 == 0) step_mark(d, 2);
+    const int ni = sl.counters[1];
+    if (split3) spread_items<P, true>(sl, ni, nry, L, Lp, s0, s1, s2);
+    else spread_items<P, false>(sl, ni, nry, L, Lp, s0, s1, s2);
     __syncthreads();
-    step_mark(d, 3);
+    if (tid < 2) sl.counters[tid] = 0;
+    __syncthreads();
   }
+  step_mark(d, 3);
   // the other parity's counters are cleared for the next launch by the system's first block
   if (tile == 0) {
     for (int j = tid; j < nbins; j += kThreads) d.bin_count[(1 - parity) * nbins + j] = 0;
     if (tid == 0) d.ovf_count[1 - parity] = 0;
   }
-  __syncthreads();
   // rows: r = ry + nry*rz (r < nry*nrz valid); FFT line t = r
   for (int idx = tid; idx < rows * L; idx += kThreads) {
     const int t = fdiv(idx, plan.n_div), e = idx - t * L;
+    const int a = t * Lp + e;
     // split: p0 + p1 2^16 + p2 2^32; carry form: s0 = lo, s1 = 0, s2 = hi -- one formula
-    const unsigned long long u = (unsigned long long)s0[idx] + ((unsigned long long)s1[idx] << 16) +
-                                 ((unsigned long long)(unsigned int)s2[idx] << 32);
+    const unsigned long long u = (unsigned long long)s0[a] + ((unsigned long long)s1[a] << 16) +
+                                 ((unsigned long long)(unsigned int)s2[a] << 32);
     b0[e * ld + t] = make_float2(fixed_to_float((long long)u), 0.0f);
   }
   __syncthreads();
@@ -845,10 +969,8 @@ __device__ __forceinline__ void finalize_system(const SysDesc& d, bool solve, bo
 // F_d = q ccelec n_d r_d sum(...) (gradient convention, CudaPMERecip.cu:1234-1242).
 // ---------------------------------------------------------------------------------------------
 template <int P, int KIND>
-__device__ __forceinline__ void gather_tile(const SysDesc& d, int tile) {
+__device__ __forceinline__ void gather_atom(const SysDesc& d, int atom, bool valid, int gl) {
   const Geom& g = d.g;
-  const int atom = tile * 32 + (threadIdx.x >> 3), gl = threadIdx.x & 7;
-  const bool valid = atom < d.natom;
   const float4 a = valid ? __ldg(&d.xyzq[atom]) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
   int ix, iy, iz;
   float ux, uy, uz;
@@ -919,6 +1041,40 @@ __device__ __forceinline__ void gather_tile(const SysDesc& d, int tile) {
   }
 }
 
+template <int P, int KIND>
+__device__ __forceinline__ void gather_tile(const SysDesc& d, int tile) {
+  const int atom = tile * 32 + (threadIdx.x >> 3), gl = threadIdx.x & 7;
+  gather_atom<P, KIND>(d, atom, atom < d.natom, gl);
+}
+
+// Fused path: gather the atoms of one row-block bin (plus the overflow atoms whose origin lies in
+// the block), 32 at a time, so that the tile's stencil rows (about (4+P-1)^2 grid rows) stay in L1.
+template <int P, int KIND>
+__device__ __forceinline__ void gather_bin_tile(const SysDesc& d, int tile, int parity) {
+  constexpr int RF = rec_floats(P);
+  const int nbins = d.nby * d.nbz;
+  const int cnt = min(__ldcg(&d.bin_count[parity * nbins + tile]), d.bin_cap);
+  const float* list = d.bin_recs + (size_t)tile * d.bin_cap * RF;
+  const int gl = threadIdx.x & 7, slot = threadIdx.x >> 3;
+  for (int j0 = 0; j0 < cnt; j0 += 32) {
+    const int j = j0 + slot;
+    const bool valid = j < cnt;
+    gather_atom<P, KIND>(d, valid ? __float_as_int(__ldcg(&list[(size_t)j * RF + 3])) : 0, valid, gl);
+  }
+  const int novf = __ldcg(&d.ovf_count[parity]);
+  for (int j0 = 0; j0 < novf; j0 += 32) {
+    const int j = j0 + slot;
+    int atom = 0;
+    bool mine = false;
+    if (j < novf) {
+      const float4 h = __ldcg((const float4*)(d.ovf_recs + (size_t)j * RF));
+      atom = __float_as_int(h.w);
+      mine = (__float_as_int(h.y) / d.bry + d.nby * (__float_as_int(h.z) / d.brz)) == tile;
+    }
+    gather_atom<P, KIND>(d, atom, mine, gl);
+  }
+}
+
 template <int P>
 __device__ __forceinline__ void gather_tile_any(const SysDesc& d, int tile) {
   switch (d.force_kind) {
@@ -933,6 +1089,23 @@ __device__ __forceinline__ void gather_dispatch(const SysDesc& d, int tile) {
     case 4: gather_tile_any<4>(d, tile); break;
     case 6: gather_tile_any<6>(d, tile); break;
     default: gather_tile_any<8>(d, tile); break;
+  }
+}
+
+template <int P>
+__device__ __forceinline__ void gather_bin_any(const SysDesc& d, int tile, int parity) {
+  switch (d.force_kind) {
+    case kForceF32Soa: gather_bin_tile<P, kForceF32Soa>(d, tile, parity); break;
+    case kForceF32x3: gather_bin_tile<P, kForceF32x3>(d, tile, parity); break;
+    default: gather_bin_tile<P, kForceI64SoaAccum>(d, tile, parity); break;
+  }
+}
+
+__device__ __forceinline__ void gather_bin_dispatch(const SysDesc& d, int tile, int parity) {
+  switch (d.order) {
+    case 4: gather_bin_any<4>(d, tile, parity); break;
+    case 6: gather_bin_any<6>(d, tile, parity); break;
+    default: gather_bin_any<8>(d, tile, parity); break;
   }
 }
 
