@@ -168,7 +168,7 @@ struct SystemState {
   int tx_rows = 0, tx_y = 0, tx_z = 0, plane = 0;
   int bry = 4, brz = 4, nby = 1, nbz = 1;
   int bin_cap = 0, atom_cap = 0;
-  int* bins = nullptr;       // [2 nbins counts][nbins*bin_cap records][2 ovf counts][atom_cap ovf records]
+  int* bins = nullptr;       // counts, bin records, bookkeeping, overflow records, atom order
   unsigned long long* accum = nullptr;
   float2* cgrid = nullptr;
   float* rgrid = nullptr;
@@ -214,12 +214,13 @@ struct SystemState {
 
   // bin storage for up to natom atoms: capacity 1.5x the mean occupancy + 32 per bin
   static int cap_for(int natom, int nbins) { return std::max(32, (int)(1.5 * natom / nbins) + 32); }
-  // counts (padded to 16 bytes), bin records, overflow counts (padded), overflow records; records
-  // are sized for order 8
+  // counts (padded to 16 bytes), bin records, bookkeeping (kMetaInts), overflow records, the
+  // bin-sorted atom order; records are sized for order 8
   size_t count_ints() const { return (2 * (size_t)nbins() + 3) & ~(size_t)3; }
   size_t bin_ints(int natom) const {
-    return count_ints() + (size_t)nbins() * cap_for(natom, nbins()) * rec_floats(kMaxOrder) + 4 +
-           (size_t)std::max(natom, 1) * rec_floats(kMaxOrder);
+    const size_t n = (size_t)std::max(natom, 1);
+    return count_ints() + (size_t)nbins() * cap_for(natom, nbins()) * rec_floats(kMaxOrder) + kMetaInts +
+           n * rec_floats(kMaxOrder) + n;
   }
 
   void carve(char* base) {
@@ -309,8 +310,9 @@ struct SystemState {
       const size_t nb = nbins();
       d.bin_count = bins;
       d.bin_recs = (float*)(bins + count_ints());
-      d.ovf_count = (int*)(d.bin_recs + nb * (size_t)bin_cap * rec_floats(kMaxOrder));
-      d.ovf_recs = (float*)(d.ovf_count + 4);
+      d.bin_meta = (int*)(d.bin_recs + nb * (size_t)bin_cap * rec_floats(kMaxOrder));
+      d.ovf_recs = (float*)(d.bin_meta + kMetaInts);
+      d.perm = (int*)(d.ovf_recs + (size_t)std::max(atom_cap, 1) * rec_floats(kMaxOrder));
     }
     return d;
   }

@@ -218,7 +218,7 @@ __global__ void __launch_bounds__(kThreads) k_fused(FusedArgs a) {
           if (local < tiles_xpass(d)) x_inv_tile(d, local, smem);
           else if (threadIdx.x == 0) finalize_system(d, true, true);
           break;
-        default: gather_bin_dispatch(d, local, parity); break;
+        default: gather_bin_dispatch(d, local, parity, (char*)smem, a.gather_wide != 0); break;
       }
       __syncthreads();
     }
@@ -327,6 +327,7 @@ cudaError_t staged_gather(const SysDesc& d, cudaStream_t s) {
 
 cudaError_t fused_launch(const FusedArgs& a, int grid, size_t smem, cudaStream_t s) {
   FusedArgs args = a;
+  args.gather_wide = a.total[kPhases - 1] <= grid ? 1 : 0;
   void* params[] = {&args};
   return cudaLaunchCooperativeKernel((const void*)k_fused, dim3(grid), dim3(kThreads), params, smem, s);
 }

@@ -29,6 +29,9 @@ enum AccSlot { kAccE = 0, kAccV0 = 1, kAccQ2 = 7, kAccCount = 8 };
 // Energy/virial record layout in device memory (doubles), as include/pme_recip.h.
 enum EvSlot { kEvRecip = 0, kEvSelf = 1, kEvVirial = 2, kEvCount = 11 };
 
+// Per-system bin bookkeeping (SysDesc::bin_meta).
+enum BinMeta { kMetaOvf = 0, kMetaQmax = 2, kMetaPermNatom = 4, kMetaInts = 8 };
+
 // Everything a tile needs to know about one system.
 struct SysDesc {
   Geom g;
@@ -63,8 +66,10 @@ struct SysDesc {
   int bin_cap;
   int* bin_count;            // [2][nby*nbz]
   float* bin_recs;           // [nby*nbz][bin_cap] atom records of rec_floats(order) floats
-  int* ovf_count;            // [2]
+  int* bin_meta;             // [8]: overflow counts [2] and max |q| as float bits [2] by launch
+                             // parity, the atom count the bin-sorted order was built for
   float* ovf_recs;           // [natom capacity] records of the atoms beyond a bin's capacity
+  int* perm;                 // [natom capacity] bin-sorted atom order of the previous evaluation
   unsigned long long* steps; // profiling: %globaltimer at the steps of CTA 0's tiles (or null)
 };
 
@@ -86,7 +91,14 @@ __host__ __device__ inline int tiles_zpass(const SysDesc& d) { return ((d.g.ny +
 __host__ __device__ inline int tiles_plane(const SysDesc& d) { return d.g.hx; }
 __host__ __device__ inline int tiles_bin(const SysDesc& d) { return (d.natom + kThreads - 1) / kThreads; }
 __host__ __device__ inline int tiles_blocks(const SysDesc& d) { return d.nby * d.nbz; }
-__host__ __device__ inline int tiles_gather(const SysDesc& d) { return (d.natom + 31) / 32; }
+// Lanes per atom of the latency-oriented gather (staged gather, fused launches with about one
+// gather tile per CTA): as few as keep the rows of one lane, P^2 / lanes, at 8-9.
+__host__ __device__ constexpr int gather_lanes(int order) { return order <= 4 ? 2 : (order <= 6 ? 4 : 8); }
+constexpr int kGatherAtoms = kThreads / 8;   // staged gather tile: atoms of the smallest pass
+__host__ __device__ inline int tiles_gather(const SysDesc& d) {
+  const int app = kThreads / gather_lanes(d.order);
+  return (d.natom + app - 1) / app;
+}
 __host__ inline size_t tile_smem_bytes(int L, int tx) {
   return sizeof(float2) * ((size_t)L + 2 * (size_t)L * (tx + 1));
 }
@@ -557,55 +569,88 @@ __device__ __forceinline__ void plane_tile(const SysDesc& d, int kx, float2* sme
 
 // ---------------------------------------------------------------------------------------------
 // Fused path, phase 0: bin kThreads atoms by the row block of their stencil origin; sum q^2.
-// A bin entry is the atom's record: stencil origin (ix, iy, iz as int bits) and atom index, then
-// the FP32 spreading weights q*thx[P], thy[P], thz[P] -- the values the staged spread uses --
-// padded to a multiple of 4 floats so that every record is 16-byte aligned.
+// A bin entry is the atom's record: stencil origin (ix, iy, iz as int bits) and atom index; the
+// FP32 spreading weights q*thx[P], thy[P], thz[P] (the values the staged spread uses), padded to a
+// multiple of 4 floats; then the fractional offsets ux, uy, uz and q for the gather.  Records are
+// 16-byte aligned.
 // ---------------------------------------------------------------------------------------------
-__host__ __device__ constexpr int rec_floats(int order) { return (4 + 3 * order + 3) & ~3; }
+__host__ __device__ constexpr int rec_floats(int order) { return ((4 + 3 * order + 3) & ~3) + 4; }
 
 template <int P>
 __device__ __forceinline__ void bin_tile_p(const SysDesc& d, int tile, int parity, long long* red) {
   constexpr int RF = rec_floats(P);
+  constexpr int NW = RF - 8;                   // weight floats incl. padding
   const Geom& g = d.g;
-  const int i = tile * kThreads + threadIdx.x;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int idx = tile * kThreads + threadIdx.x;
+  const bool valid = idx < d.natom;
   const int nbins = d.nby * d.nbz;
+  // walk the atoms in the previous evaluation's bin-sorted order when it is one for this count
+  const bool sorted = __ldcg(&d.bin_meta[kMetaPermNatom]) == d.natom;
+  const int i = valid && sorted ? __ldcg(&d.perm[idx]) : idx;
+  step_mark(d, 16);
   long long q2 = 0;
-  if (i < d.natom) {
+  unsigned int qbits = 0u;
+  int b = -1, ix = 0, iy = 0, iz = 0;
+  float ux = 0.0f, uy = 0.0f, uz = 0.0f, q = 0.0f;
+  float w[NW];
+#pragma unroll
+  for (int k = 0; k < NW; k++) w[k] = 0.0f;
+  if (valid) {
     const float4 a = __ldg(&d.xyzq[i]);
-    int ix, iy, iz;
-    float ux, uy, uz;
     frac_coord(a.x, g.sx_hi, g.sx_lo, g.nx, ix, ux);
     frac_coord(a.y, g.sy_hi, g.sy_lo, g.ny, iy, uy);
     frac_coord(a.z, g.sz_hi, g.sz_lo, g.nz, iz, uz);
-    float w[RF - 4];
-#pragma unroll
-    for (int k = 3 * P; k < RF - 4; k++) w[k] = 0.0f;
     bspline<P>(ux, w, nullptr);
 #pragma unroll
     for (int k = 0; k < P; k++) w[k] = __fmul_rn(a.w, w[k]);
     bspline<P>(uy, w + P, nullptr);
     bspline<P>(uz, w + 2 * P, nullptr);
-    const int b = iy / d.bry + d.nby * (iz / d.brz);
-    const int slot = atomicAdd(&d.bin_count[parity * nbins + b], 1);
+    q = a.w;
+    b = iy / d.bry + d.nby * (iz / d.brz);
+    q2 = q2_fixed(a.w);
+    qbits = (unsigned int)__float_as_int(fabsf(a.w));
+  }
+  step_mark(d, 17);
+  // slots: one counter update per group of lanes with the same bin
+  const unsigned int grp = __match_any_sync(0xffffffffu, b);
+  const int leader = __ffs(grp) - 1;
+  int base = 0;
+  if (valid && lane == leader) base = atomicAdd(&d.bin_count[parity * nbins + b], __popc(grp));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  step_mark(d, 18);
+  if (valid) {
+    const int slot = base + __popc(grp & ((1u << lane) - 1u));
     float* rec;
     if (slot < d.bin_cap) {
       rec = d.bin_recs + ((size_t)b * d.bin_cap + slot) * RF;
     } else {
-      const int o = atomicAdd(&d.ovf_count[parity], 1);
+      const int o = atomicAdd(&d.bin_meta[kMetaOvf + parity], 1);
       rec = d.ovf_recs + (size_t)o * RF;
     }
     float4* r4 = (float4*)rec;
     __stcg(&r4[0], make_float4(__int_as_float(ix), __int_as_float(iy), __int_as_float(iz), __int_as_float(i)));
 #pragma unroll
-    for (int c = 0; c < (RF - 4) / 4; c++)
+    for (int c = 0; c < NW / 4; c++)
       __stcg(&r4[1 + c], make_float4(w[4 * c], w[4 * c + 1], w[4 * c + 2], w[4 * c + 3]));
-    q2 = q2_fixed(a.w);
+    __stcg(&r4[RF / 4 - 1], make_float4(ux, uy, uz, q));
   }
-  if (d.calc_self) {
-    const long long sum = block_sum_ll(q2, red);
-    if (threadIdx.x == 0 && sum != 0) atomicAdd((unsigned long long*)&d.acc[kAccQ2], (unsigned long long)sum);
+  step_mark(d, 19);
+  // max |q| of the system (float bits of non-negative values order as integers) and sum q^2
+  qbits = __reduce_max_sync(0xffffffffu, qbits);
+  unsigned int* qs = (unsigned int*)(red + 16);
+  if (lane == 0) qs[warp] = qbits;
+  const long long sum = block_sum_ll(q2, red);
+  if (threadIdx.x == 0) {
+    unsigned int m = 0u;
+#pragma unroll
+    for (int k = 0; k < kThreads / 32; k++) m = max(m, qs[k]);
+    if (m != 0u) atomicMax((unsigned int*)&d.bin_meta[kMetaQmax + parity], m);
+    if (d.calc_self && sum != 0) atomicAdd((unsigned long long*)&d.acc[kAccQ2], (unsigned long long)sum);
   }
+  step_mark(d, 20);
   __syncthreads();
+  step_mark(d, 21);
 }
 
 __device__ __forceinline__ void bin_tile(const SysDesc& d, int tile, int parity, long long* red) {
@@ -648,29 +693,44 @@ __host__ __device__ inline size_t spread_x_smem_bytes(int nx, int rows, int orde
   return acc + align16((size_t)nx * sizeof(float2)) + kSpreadBookInts * sizeof(int) + (fft > lists ? fft : lists);
 }
 
-// Exact int64 accumulation in shared memory with native 32-bit atomics.  A contribution
-// v = p0 + p1 2^16 + p2 2^32 (p0, p1 in [0, 2^16), p2 = v >> 32 signed) is added to three 32-bit
-// sums without using the atomics' return values (no dependent round trips).  The p0 and p1 sums
-// cannot wrap while a point receives at most 2^16 contributions, which the tile guarantees by
-// checking its candidate count; the p2 sum may wrap, harmlessly, since only its value modulo 2^32
-// enters the int64 result.  Beyond that count the carry form is used: lo (u32) + hi (s32), the
-// wrap of lo detected from the returned old value.
-__device__ __forceinline__ void add_fixed_split3(unsigned int* s0, unsigned int* s1, int* s2, int idx,
-                                                 long long v) {
-  const unsigned long long u = (unsigned long long)v;
-  const unsigned int p0 = (unsigned int)(u & 0xffffull), p1 = (unsigned int)((u >> 16) & 0xffffull);
-  const int p2 = (int)(v >> 32);
-  atomicAdd(&s0[idx], p0);
-  atomicAdd(&s1[idx], p1);
-  if (p2 != 0) atomicAdd(&s2[idx], p2);
-}
+// Exact int64 accumulation in shared memory with native 32-bit atomics, in one of three forms
+// chosen per tile before its first contribution.  A point receives at most one contribution per
+// candidate atom (the P stencil points of an axis are distinct), so with n candidates:
+//  split2(k): v = lo + hi 2^k, lo = v mod 2^k in [0, 2^k), hi = v >> k (signed): two sums.  The
+//    lo sum stays below n 2^k <= 2^32; the hi sum's magnitude below n (|v|max / 2^k + 1), where
+//    |v| <= |q| 2^40 because every spline weight is at most 1.  k is the largest value with
+//    n 2^k < 2^32, and the form is taken when the hi bound, from the system's max |q|, is below
+//    2^31.
+//  split3: v = p0 + p1 2^16 + p2 2^32 (p0, p1 in [0, 2^16), p2 = v >> 32): the p0 and p1 sums
+//    cannot wrap for n <= 2^16; the p2 sum may wrap, harmlessly, since only its value modulo 2^32
+//    enters the int64 result.
+//  carry: lo (u32) + hi (s32), the wrap of lo detected from the returned old value (any n).
+// Only the carry form waits for an atomic's result.  In every form the point's value is
+// s0 + s1 2^16 + s2 2^sh (s2 sign-extended; sh = k for split2, 32 otherwise) modulo 2^64.
+enum SpreadMode { kSplit2 = 0, kSplit3 = 1, kCarry = 2 };
 
-__device__ __forceinline__ void add_fixed_carry(unsigned int* lo, int* hi, int idx, long long v) {
-  const unsigned int l = (unsigned int)(unsigned long long)v;
-  const int h = (int)(v >> 32);
-  const unsigned int old = atomicAdd(&lo[idx], l);
-  const int carry = (old + l) < old ? 1 : 0;
-  if (h + carry != 0) atomicAdd(&hi[idx], h + carry);
+template <int MODE>
+__device__ __forceinline__ void add_fixed(unsigned int* s0, unsigned int* s1, int* s2, int idx, long long v,
+                                          int k, unsigned int kmask) {
+  if (MODE == kSplit2) {
+    const unsigned int lo = (unsigned int)(unsigned long long)v & kmask;
+    const int hi = (int)(v >> k);
+    atomicAdd(&s0[idx], lo);
+    if (hi != 0) atomicAdd(&s2[idx], hi);
+  } else if (MODE == kSplit3) {
+    const unsigned long long u = (unsigned long long)v;
+    const unsigned int p0 = (unsigned int)(u & 0xffffull), p1 = (unsigned int)((u >> 16) & 0xffffull);
+    const int p2 = (int)(v >> 32);
+    atomicAdd(&s0[idx], p0);
+    atomicAdd(&s1[idx], p1);
+    if (p2 != 0) atomicAdd(&s2[idx], p2);
+  } else {
+    const unsigned int l = (unsigned int)(unsigned long long)v;
+    const int h = (int)(v >> 32);
+    const unsigned int old = atomicAdd(&s0[idx], l);
+    const int carry = (old + l) < old ? 1 : 0;
+    if (h + carry != 0) atomicAdd(&s2[idx], h + carry);
+  }
 }
 
 // The listed atoms of a round, structure of arrays over kSpreadSlots slots:
@@ -684,22 +744,38 @@ struct SpreadLists {
   int* counters;   // [0] listed atoms, [1] items
 };
 
-// Step A for one candidate record per lane (rec == nullptr: no candidate).  Every lane of the
-// warp calls it.
+// First candidate bin and number of candidate bins along one axis: the origin rows
+// R0-P+1 .. R0+nr-1 (wrapped) cover the consecutive bins b0, b0+1, ..., own (mod nb), or every
+// bin when the window spans the axis.  At most ceil((P-1)/br) + 2 <= 8 bins.
+__device__ __forceinline__ void cand_axis(int P, int n, int br, int nb, int own, int R0, int nr, int& b0, int& cnt) {
+  if (P - 1 + nr >= n) {
+    b0 = 0;
+    cnt = nb;
+    return;
+  }
+  int r0 = (R0 - P + 1) % n;
+  if (r0 < 0) r0 += n;
+  b0 = r0 / br;
+  cnt = own - b0;
+  if (cnt < 0) cnt += nb;
+  cnt += 1;
+}
+
+// Step A for one candidate per lane, its record already loaded (has == false: no candidate).
+// Every lane of the warp calls it.
 template <int P>
-__device__ __forceinline__ void spread_list_atom(const SysDesc& d, const float* rec, int Y0, int Z0, int nry,
-                                                 int nrz, const SpreadLists& sl) {
+__device__ __forceinline__ void spread_list_atom(const SysDesc& d, bool has, const float4& head,
+                                                 const float4 (&w4)[(rec_floats(P) - 8) / 4], int Y0, int Z0,
+                                                 int nry, int nrz, const SpreadLists& sl) {
   constexpr int S = kSpreadSlots;
   const Geom& g = d.g;
   const int lane = threadIdx.x & 31;
   unsigned int my = 0u, mz = 0u;   // block rows covered by the stencil
-  int ix = 0, ry0 = 0, rz0 = 0;
-  if (rec != nullptr) {
-    const float4 h = __ldcg((const float4*)rec);
-    ix = __float_as_int(h.x);
-    ry0 = __float_as_int(h.y) - Y0;
+  int ry0 = 0, rz0 = 0;
+  if (has) {
+    ry0 = __float_as_int(head.y) - Y0;
     if (ry0 < 0) ry0 += g.ny;
-    rz0 = __float_as_int(h.z) - Z0;
+    rz0 = __float_as_int(head.z) - Z0;
     if (rz0 < 0) rz0 += g.nz;
 #pragma unroll
     for (int b = 0; b < P; b++) {
@@ -730,18 +806,16 @@ __device__ __forceinline__ void spread_list_atom(const SysDesc& d, const float* 
   ibase = __shfl_sync(0xffffffffu, ibase, 0);
   if (nrow == 0) return;
   const int slot = sbase + __popc(act & ((1u << lane) - 1u));
-  constexpr int NW = rec_floats(P) - 4;
+  constexpr int NW = rec_floats(P) - 8;
   float w[NW];
-  const float4* r4 = (const float4*)rec + 1;
 #pragma unroll
   for (int c = 0; c < NW / 4; c++) {
-    const float4 v = __ldcg(&r4[c]);
-    w[4 * c] = v.x;
-    w[4 * c + 1] = v.y;
-    w[4 * c + 2] = v.z;
-    w[4 * c + 3] = v.w;
+    w[4 * c] = w4[c].x;
+    w[4 * c + 1] = w4[c].y;
+    w[4 * c + 2] = w4[c].z;
+    w[4 * c + 3] = w4[c].w;
   }
-  sl.ix[slot] = ix;
+  sl.ix[slot] = __float_as_int(head.x);
 #pragma unroll
   for (int k = 0; k < P; k++) sl.w[k * S + slot] = w[k];
 #pragma unroll
@@ -768,9 +842,10 @@ __device__ __forceinline__ void spread_list_atom(const SysDesc& d, const float* 
 }
 
 // Step B: the P contributions of one (atom, block row) item per lane.
-template <int P, bool SPLIT3>
+template <int P, int MODE>
 __device__ __forceinline__ void spread_items(const SpreadLists& sl, int nitems, int nry, int L, int Lp,
-                                             unsigned int* s0, unsigned int* s1, int* s2) {
+                                             unsigned int* s0, unsigned int* s1, int* s2, int k2,
+                                             unsigned int kmask) {
   constexpr int S = kSpreadSlots;
   for (int j = threadIdx.x; j < nitems; j += kThreads) {
     const unsigned int it = sl.items[j];
@@ -783,9 +858,7 @@ __device__ __forceinline__ void spread_items(const SpreadLists& sl, int nitems, 
     for (int k = 0; k < P; k++) {
       int x = ix + k;
       if (x >= L) x -= L;
-      const long long v = fixed_contrib(sl.w[k * S + slot], ty, tz);
-      if (SPLIT3) add_fixed_split3(s0, s1, s2, rb + x, v);
-      else add_fixed_carry(s0, s2, rb + x, v);
+      add_fixed<MODE>(s0, s1, s2, rb + x, fixed_contrib(sl.w[k * S + slot], ty, tz), k2, kmask);
     }
   }
 }
@@ -793,7 +866,9 @@ __device__ __forceinline__ void spread_items(const SpreadLists& sl, int nitems, 
 template <int P>
 __device__ __forceinline__ void spread_x_tile(const SysDesc& d, int tile, int parity, char* smem_raw) {
   constexpr int RF = rec_floats(P);
+  constexpr int NW4 = (RF - 8) / 4;          // float4s of spreading weights
   constexpr int S = kSpreadSlots;
+  constexpr int PRE = P <= 4 ? 2 : 1;          // candidates whose records a thread loads at once
   const Geom& g = d.g;
   const FftPlan1D& plan = d.px;
   const int L = g.nx, Lp = spread_row_stride(L);
@@ -809,90 +884,111 @@ __device__ __forceinline__ void spread_x_tile(const SysDesc& d, int tile, int pa
   char* p = smem_raw + align16((size_t)rows * Lp * 12);
   float2* tw = (float2*)p;
   p += align16((size_t)L * sizeof(float2));
-  int* cand = (int*)p;                         // [0..7] y bins, [8..15] z bins, [16] #y, [17] #z
-  int* ccnt = cand + 32;                       // [64] counts of the candidate bins
-  int* coff = ccnt + 64;                       // [65] their offsets
+  int* book = (int*)p;                         // [0..1] counters, [32..96] candidate-bin offsets
+  int* coff = book + 32;
   p += kSpreadBookInts * sizeof(int);
   SpreadLists sl;
   sl.ix = (int*)p;
   sl.w = (float*)(sl.ix + S);
   sl.items = (unsigned short*)(sl.w + (size_t)(P + 2 * kSpreadMaxBlock) * S);
-  sl.counters = cand + 18;
+  sl.counters = book;
   float2* b0 = (float2*)p;                     // FFT view of the work area (after spreading)
   float2* b1 = b0 + (size_t)L * ld;
   const int nbins = d.nby * d.nbz;
   step_mark(d, 0);
+  // twiddles: loaded now, stored to smem once the spreading is done (L <= 2 kThreads)
+  const float2 tw0 = tid < L ? __ldg(&d.tw[plan.tw_off + tid]) : make_float2(0.0f, 0.0f);
+  const float2 tw1 = tid + kThreads < L ? __ldg(&d.tw[plan.tw_off + tid + kThreads]) : make_float2(0.0f, 0.0f);
+  int b0y, ncy, b0z, ncz;
+  cand_axis(P, g.ny, d.bry, d.nby, by, Y0, nry, b0y, ncy);
+  cand_axis(P, g.nz, d.brz, d.nbz, bz, Z0, nrz, b0z, ncz);
+  const int nc = ncy * ncz;
+  if (tid < 32) {
+    // counts of the candidate bins (c = cy + ncy cz, at most 64) and their exclusive prefix
+    int n01[2], inc[2];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const int c = tid + 32 * h;
+      n01[h] = 0;
+      if (c < nc) {
+        int cby = b0y + c % ncy, cbz = b0z + c / ncy;
+        if (cby >= d.nby) cby -= d.nby;
+        if (cbz >= d.nbz) cbz -= d.nbz;
+        n01[h] = min(__ldcg(&d.bin_count[parity * nbins + cby + d.nby * cbz]), d.bin_cap);
+      }
+      inc[h] = n01[h];
+    }
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const int t = __shfl_up_sync(0xffffffffu, inc[h], o);
+        if (tid >= o) inc[h] += t;
+      }
+    }
+    const int tot0 = __shfl_sync(0xffffffffu, inc[0], 31);
+    coff[tid] = inc[0] - n01[0];
+    coff[tid + 32] = tot0 + inc[1] - n01[1];
+    if (tid == 31) coff[64] = tot0 + inc[1];
+    if (tid < 2) sl.counters[tid] = 0;
+  }
   for (int idx = tid; idx < rows * Lp; idx += kThreads) {
     s0[idx] = 0u;
     s1[idx] = 0u;
     s2[idx] = 0;
   }
-  for (int i = tid; i < L; i += kThreads) tw[i] = __ldg(&d.tw[plan.tw_off + i]);
-  // Candidate bins: the origin rows Y0-P+1 .. Y0+nry-1 (wrapped) cover consecutive bins
-  // b0, b0+1, ..., by (mod nby); all bins when the window spans the whole axis.  Same for z.
-  // At most ceil((P-1)/bry) + 2 <= 8 bins per axis.
-  if (tid < 2) {
-    const int n = tid == 0 ? g.ny : g.nz, br = tid == 0 ? d.bry : d.brz;
-    const int nb = tid == 0 ? d.nby : d.nbz, own = tid == 0 ? by : bz;
-    const int R0 = tid == 0 ? Y0 : Z0, nr = tid == 0 ? nry : nrz;
-    const int W = P - 1 + nr;
-    int* out = cand + 8 * tid;
-    if (W >= n) {
-      for (int k = 0; k < nb; k++) out[k] = k;
-      cand[16 + tid] = nb;
-    } else {
-      int r0 = (R0 - P + 1) % n;
-      if (r0 < 0) r0 += n;
-      const int b0 = r0 / br;
-      int cnt = own - b0;
-      if (cnt < 0) cnt += nb;
-      cnt += 1;
-      for (int k = 0; k < cnt; k++) {
-        const int b = b0 + k;
-        out[k] = b >= nb ? b - nb : b;
-      }
-      cand[16 + tid] = cnt;
-    }
-    sl.counters[tid] = 0;
-  }
-  __syncthreads();
-  const int ncy = cand[16], ncz = cand[17], nc = ncy * ncz;
-  if (tid < nc) {
-    const int b = cand[tid % ncy] + d.nby * cand[8 + tid / ncy];
-    ccnt[tid] = min(__ldcg(&d.bin_count[parity * nbins + b]), d.bin_cap);
-  }
-  __syncthreads();
-  if (tid == 0) {
-    int o = 0;
-    for (int c = 0; c < nc; c++) { coff[c] = o; o += ccnt[c]; }
-    coff[nc] = o;
-  }
+  const int novf = __ldcg(&d.bin_meta[kMetaOvf + parity]);
+  const float qmax = __int_as_float(__ldcg(&d.bin_meta[kMetaQmax + parity]));
   __syncthreads();
   const int total = coff[nc];
   step_mark(d, 1);
-  const int ncand = total + __ldcg(&d.ovf_count[parity]);
-  // at most one contribution per candidate and point: up to 2^16 candidates the split form is exact
-  const bool split3 = ncand <= 65536;
+  const int ncand = total + novf;
+  // accumulation form for this tile (see add_fixed)
+  const int k2 = __clz(max(ncand, 1));          // largest k with ncand 2^k < 2^32
+  const unsigned int kmask = (unsigned int)((1ull << k2) - 1ull);
+  const double hib = (double)ncand * ((double)qmax * ldexp(1.0, 40 - k2) * 1.001 + 2.0);
+  const int mode = hib < 2147483648.0 ? kSplit2 : (ncand <= 65536 ? kSplit3 : kCarry);
   for (int base0 = 0; base0 < ncand; base0 += S) {
 #pragma unroll 1
-    for (int h = 0; h < S; h += kThreads) {
-      const int q = base0 + h + tid;
-      const float* rec = nullptr;
-      if (q < total) {
-        int c = 0;
-        while (q >= coff[c + 1]) c++;
-        const int b = cand[c % ncy] + d.nby * cand[8 + c / ncy];
-        rec = d.bin_recs + ((size_t)b * d.bin_cap + (q - coff[c])) * RF;
-      } else if (q < ncand) {
-        rec = d.ovf_recs + (size_t)(q - total) * RF;
+    for (int h0 = 0; h0 < S; h0 += PRE * kThreads) {
+      bool has[PRE];
+      float4 head[PRE];
+      float4 w4[PRE][NW4];
+#pragma unroll
+      for (int u = 0; u < PRE; u++) {
+        const int q = base0 + h0 + u * kThreads + tid;
+        const float* rec = nullptr;
+        if (q < total) {
+          int c = 0;
+          while (q >= coff[c + 1]) c++;
+          int cby = b0y + c % ncy, cbz = b0z + c / ncy;
+          if (cby >= d.nby) cby -= d.nby;
+          if (cbz >= d.nbz) cbz -= d.nbz;
+          rec = d.bin_recs + ((size_t)(cby + d.nby * cbz) * d.bin_cap + (q - coff[c])) * RF;
+        } else if (q < ncand) {
+          rec = d.ovf_recs + (size_t)(q - total) * RF;
+        }
+        has[u] = rec != nullptr;
+        if (has[u]) {
+          const float4* r4 = (const float4*)rec;
+          head[u] = __ldcg(r4);
+#pragma unroll
+          for (int c = 0; c < NW4; c++) w4[u][c] = __ldcg(r4 + 1 + c);
+        } else {
+          head[u] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+#pragma unroll
+          for (int c = 0; c < NW4; c++) w4[u][c] = head[u];
+        }
       }
-      spread_list_atom<P>(d, rec, Y0, Z0, nry, nrz, sl);
+#pragma unroll
+      for (int u = 0; u < PRE; u++) spread_list_atom<P>(d, has[u], head[u], w4[u], Y0, Z0, nry, nrz, sl);
     }
     __syncthreads();
     if (base0 == 0) step_mark(d, 2);
     const int ni = sl.counters[1];
-    if (split3) spread_items<P, true>(sl, ni, nry, L, Lp, s0, s1, s2);
-    else spread_items<P, false>(sl, ni, nry, L, Lp, s0, s1, s2);
+    if (mode == kSplit2) spread_items<P, kSplit2>(sl, ni, nry, L, Lp, s0, s1, s2, k2, kmask);
+    else if (mode == kSplit3) spread_items<P, kSplit3>(sl, ni, nry, L, Lp, s0, s1, s2, k2, kmask);
+    else spread_items<P, kCarry>(sl, ni, nry, L, Lp, s0, s1, s2, k2, kmask);
     __syncthreads();
     if (tid < 2) sl.counters[tid] = 0;
     __syncthreads();
@@ -901,15 +997,17 @@ __device__ __forceinline__ void spread_x_tile(const SysDesc& d, int tile, int pa
   // the other parity's counters are cleared for the next launch by the system's first block
   if (tile == 0) {
     for (int j = tid; j < nbins; j += kThreads) d.bin_count[(1 - parity) * nbins + j] = 0;
-    if (tid == 0) d.ovf_count[1 - parity] = 0;
+    if (tid < 2) d.bin_meta[2 * tid + 1 - parity] = 0;   // overflow count, max |q|
   }
+  if (tid < L) tw[tid] = tw0;
+  if (tid + kThreads < L) tw[tid + kThreads] = tw1;
+  const int sh = mode == kSplit2 ? k2 : 32;
   // rows: r = ry + nry*rz (r < nry*nrz valid); FFT line t = r
   for (int idx = tid; idx < rows * L; idx += kThreads) {
     const int t = fdiv(idx, plan.n_div), e = idx - t * L;
     const int a = t * Lp + e;
-    // split: p0 + p1 2^16 + p2 2^32; carry form: s0 = lo, s1 = 0, s2 = hi -- one formula
     const unsigned long long u = (unsigned long long)s0[a] + ((unsigned long long)s1[a] << 16) +
-                                 ((unsigned long long)(unsigned int)s2[a] << 32);
+                                 ((unsigned long long)(long long)s2[a] << sh);
     b0[e * ld + t] = make_float2(fixed_to_float((long long)u), 0.0f);
   }
   __syncthreads();
@@ -964,11 +1062,108 @@ __device__ __forceinline__ void finalize_system(const SysDesc& d, bool solve, bo
 }
 
 // ---------------------------------------------------------------------------------------------
-// Gather tile: 32 atoms, 8 lanes per atom; lane l takes stencil rows (b, c) = l, l+8, ... of the
-// P^2 rows and sums the P points of each row; the 8 partial sums are combined with shuffles.
+// Gather of one atom by LPA lanes (2, 4 or 8).  The P^2 stencil rows (b, c), r = b + P c, fall
+// into 8 groups r mod 8; each group's rows are summed in order of r, then the 8 group sums are
+// combined by the same pairwise tree whatever LPA is (groups g and g^4, then g^2, then g^1), the
+// pairs on one lane added locally and the others by shuffles.  Every LPA therefore gives the same
+// bits, so the staged and the fused gather agree however many lanes each gives an atom.
 // F_d = q ccelec n_d r_d sum(...) (gradient convention, CudaPMERecip.cu:1234-1242).
-// ---------------------------------------------------------------------------------------------
-template <int P, int KIND>
+template <int P>
+struct GatherSplines {
+  float thx[P], dthx[P], thy[P], dthy[P], thz[P], dthz[P];
+  int xs[P];
+};
+
+// Sum of the rows r = g, g+8, g+16, ... < P^2 (group g) for the three force components.
+template <int P>
+__device__ __forceinline__ float3 gather_group(const SysDesc& d, const GatherSplines<P>& sp, int g, int iy, int iz,
+                                               bool valid) {
+  const Geom& gm = d.g;
+  constexpr int RPG = (P * P + 7) / 8;
+  float f1 = 0.0f, f2 = 0.0f, f3 = 0.0f;
+#pragma unroll
+  for (int rr = 0; rr < RPG; rr++) {
+    const int r = g + 8 * rr;
+    if (valid && r < P * P) {
+      const int b = r % P, c = r / P;
+      float wy = 0.0f, dwy = 0.0f, wz = 0.0f, dwz = 0.0f;
+#pragma unroll
+      for (int q = 0; q < P; q++) {
+        if (q == b) { wy = sp.thy[q]; dwy = sp.dthy[q]; }
+        if (q == c) { wz = sp.thz[q]; dwz = sp.dthz[q]; }
+      }
+      const int y = wrap_add(iy, b, gm.ny), z = wrap_add(iz, c, gm.nz);
+      const float* row = d.rgrid + (size_t)gm.nx * (y + (size_t)gm.ny * z);
+      float s1 = 0.0f, s2 = 0.0f;
+#pragma unroll
+      for (int i = 0; i < P; i++) {
+        const float v = row[sp.xs[i]];
+        s1 = fmaf(sp.dthx[i], v, s1);
+        s2 = fmaf(sp.thx[i], v, s2);
+      }
+      f1 = fmaf(s1, wy * wz, f1);
+      f2 = fmaf(s2, dwy * wz, f2);
+      f3 = fmaf(s2, wy * dwz, f3);
+    }
+  }
+  return make_float3(f1, f2, f3);
+}
+
+__device__ __forceinline__ float3 add3(float3 a, float3 b) { return make_float3(a.x + b.x, a.y + b.y, a.z + b.z); }
+
+template <int P, int KIND, int LPA>
+__device__ __forceinline__ void gather_core(const SysDesc& d, int atom, bool valid, int gl, int ix, int iy, int iz,
+                                            float ux, float uy, float uz, float q) {
+  static_assert(LPA == 2 || LPA == 4 || LPA == 8, "lanes per atom");
+  const Geom& g = d.g;
+  GatherSplines<P> sp;
+  bspline<P>(ux, sp.thx, sp.dthx);
+  bspline<P>(uy, sp.thy, sp.dthy);
+  bspline<P>(uz, sp.thz, sp.dthz);
+#pragma unroll
+  for (int i = 0; i < P; i++) sp.xs[i] = wrap_add(ix, i, g.nx);
+  // this lane's groups gl + LPA m, combined locally in the tree's order
+  float3 f;
+  if (LPA == 8) {
+    f = gather_group<P>(d, sp, gl, iy, iz, valid);
+  } else if (LPA == 4) {
+    f = add3(gather_group<P>(d, sp, gl, iy, iz, valid), gather_group<P>(d, sp, gl + 4, iy, iz, valid));
+  } else {
+    const float3 a = add3(gather_group<P>(d, sp, gl, iy, iz, valid), gather_group<P>(d, sp, gl + 4, iy, iz, valid));
+    const float3 b = add3(gather_group<P>(d, sp, gl + 2, iy, iz, valid), gather_group<P>(d, sp, gl + 6, iy, iz, valid));
+    f = add3(a, b);
+  }
+#pragma unroll
+  for (int off = LPA / 2; off >= 1; off >>= 1) {
+    f.x += __shfl_xor_sync(0xffffffffu, f.x, off);
+    f.y += __shfl_xor_sync(0xffffffffu, f.y, off);
+    f.z += __shfl_xor_sync(0xffffffffu, f.z, off);
+  }
+  if (valid && gl == 0) {
+    const float qc = q * (float)kCcelec;
+    const float fx = qc * g.sx_hi * f.x;
+    const float fy = qc * g.sy_hi * f.y;
+    const float fz = qc * g.sz_hi * f.z;
+    const size_t st = (size_t)d.stride;
+    if (KIND == kForceF32Soa) {
+      float* fo = (float*)d.force;
+      fo[atom] = fx;
+      fo[atom + st] = fy;
+      fo[atom + 2 * st] = fz;
+    } else if (KIND == kForceF32x3) {
+      float* fo = (float*)d.force + 3 * (size_t)atom;
+      fo[0] = fx; fo[1] = fy; fo[2] = fz;
+    } else {
+      unsigned long long* fo = (unsigned long long*)d.force;
+      atomicAdd(&fo[atom], (unsigned long long)__float2ll_rn(__fmul_rn(fx, kFixedScale)));
+      atomicAdd(&fo[atom + st], (unsigned long long)__float2ll_rn(__fmul_rn(fy, kFixedScale)));
+      atomicAdd(&fo[atom + 2 * st], (unsigned long long)__float2ll_rn(__fmul_rn(fz, kFixedScale)));
+    }
+  }
+}
+
+// One atom's force from its coordinates (the staged gather).
+template <int P, int KIND, int LPA>
 __device__ __forceinline__ void gather_atom(const SysDesc& d, int atom, bool valid, int gl) {
   const Geom& g = d.g;
   const float4 a = valid ? __ldg(&d.xyzq[atom]) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
@@ -977,102 +1172,100 @@ __device__ __forceinline__ void gather_atom(const SysDesc& d, int atom, bool val
   frac_coord(a.x, g.sx_hi, g.sx_lo, g.nx, ix, ux);
   frac_coord(a.y, g.sy_hi, g.sy_lo, g.ny, iy, uy);
   frac_coord(a.z, g.sz_hi, g.sz_lo, g.nz, iz, uz);
-  float thx[P], dthx[P], thy[P], dthy[P], thz[P], dthz[P];
-  bspline<P>(ux, thx, dthx);
-  bspline<P>(uy, thy, dthy);
-  bspline<P>(uz, thz, dthz);
-  int xs[P];
-#pragma unroll
-  for (int i = 0; i < P; i++) xs[i] = wrap_add(ix, i, g.nx);
-  float f1 = 0.0f, f2 = 0.0f, f3 = 0.0f;
-  constexpr int RPL = (P * P + 7) / 8;
-  const float* rg = d.rgrid;
-#pragma unroll
-  for (int rr = 0; rr < RPL; rr++) {
-    const int r = gl + 8 * rr;
-    if (valid && r < P * P) {
-      const int b = r % P, c = r / P;
-      float wy = 0.0f, dwy = 0.0f, wz = 0.0f, dwz = 0.0f;
-#pragma unroll
-      for (int q = 0; q < P; q++) {
-        if (q == b) { wy = thy[q]; dwy = dthy[q]; }
-        if (q == c) { wz = thz[q]; dwz = dthz[q]; }
-      }
-      const int y = wrap_add(iy, b, g.ny), z = wrap_add(iz, c, g.nz);
-      const float* row = rg + (size_t)g.nx * (y + (size_t)g.ny * z);
-      float s1 = 0.0f, s2 = 0.0f;
-#pragma unroll
-      for (int i = 0; i < P; i++) {
-        const float v = row[xs[i]];
-        s1 = fmaf(dthx[i], v, s1);
-        s2 = fmaf(thx[i], v, s2);
-      }
-      f1 = fmaf(s1, wy * wz, f1);
-      f2 = fmaf(s2, dwy * wz, f2);
-      f3 = fmaf(s2, wy * dwz, f3);
-    }
-  }
-#pragma unroll
-  for (int off = 4; off >= 1; off >>= 1) {
-    f1 += __shfl_xor_sync(0xffffffffu, f1, off);
-    f2 += __shfl_xor_sync(0xffffffffu, f2, off);
-    f3 += __shfl_xor_sync(0xffffffffu, f3, off);
-  }
-  if (valid && gl == 0) {
-    const float qc = a.w * (float)kCcelec;
-    const float fx = qc * g.sx_hi * f1;
-    const float fy = qc * g.sy_hi * f2;
-    const float fz = qc * g.sz_hi * f3;
-    const size_t st = (size_t)d.stride;
-    if (KIND == kForceF32Soa) {
-      float* f = (float*)d.force;
-      f[atom] = fx;
-      f[atom + st] = fy;
-      f[atom + 2 * st] = fz;
-    } else if (KIND == kForceF32x3) {
-      float* f = (float*)d.force + 3 * (size_t)atom;
-      f[0] = fx; f[1] = fy; f[2] = fz;
-    } else {
-      unsigned long long* f = (unsigned long long*)d.force;
-      atomicAdd(&f[atom], (unsigned long long)__float2ll_rn(__fmul_rn(fx, kFixedScale)));
-      atomicAdd(&f[atom + st], (unsigned long long)__float2ll_rn(__fmul_rn(fy, kFixedScale)));
-      atomicAdd(&f[atom + 2 * st], (unsigned long long)__float2ll_rn(__fmul_rn(fz, kFixedScale)));
-    }
-  }
+  gather_core<P, KIND, LPA>(d, atom, valid, gl, ix, iy, iz, ux, uy, uz, a.w);
 }
 
 template <int P, int KIND>
 __device__ __forceinline__ void gather_tile(const SysDesc& d, int tile) {
-  const int atom = tile * 32 + (threadIdx.x >> 3), gl = threadIdx.x & 7;
-  gather_atom<P, KIND>(d, atom, atom < d.natom, gl);
+  constexpr int LPA = gather_lanes(P), APP = kThreads / LPA;
+  const int atom = tile * APP + threadIdx.x / LPA, gl = threadIdx.x % LPA;
+  if (tile * APP + (threadIdx.x >> 5) * (32 / LPA) < d.natom)   // warp-uniform
+    gather_atom<P, KIND, LPA>(d, atom, atom < d.natom, gl);
 }
 
 // Fused path: gather the atoms of one row-block bin (plus the overflow atoms whose origin lies in
-// the block), 32 at a time, so that the tile's stencil rows (about (4+P-1)^2 grid rows) stay in L1.
-template <int P, int KIND>
-__device__ __forceinline__ void gather_bin_tile(const SysDesc& d, int tile, int parity) {
+// the block), kGatherAtoms at a time, so that the tile's stencil rows (about
+// (4+P-1)^2 grid rows) stay in L1.  Atoms come from the bin's records (origin, fractional offsets
+// and charge, so no coordinate reload), the next pass's records loading while the current ones are
+// gathered.  The tile also writes its atoms into the system's bin-sorted atom order at the bin's
+// offset; the next evaluation's binning walks the atoms in that order, so that the atoms of a warp
+// share a few bins.  Overflow atoms follow all binned ones.
+template <int P, int KIND, int LPA>
+__device__ __forceinline__ void gather_bin_tile(const SysDesc& d, int tile, int parity, int* red) {
   constexpr int RF = rec_floats(P);
   const int nbins = d.nby * d.nbz;
-  const int cnt = min(__ldcg(&d.bin_count[parity * nbins + tile]), d.bin_cap);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int* counts = d.bin_count + parity * nbins;
+  const int cnt = min(__ldcg(&counts[tile]), d.bin_cap);
   const float* list = d.bin_recs + (size_t)tile * d.bin_cap * RF;
-  const int gl = threadIdx.x & 7, slot = threadIdx.x >> 3;
-  for (int j0 = 0; j0 < cnt; j0 += 32) {
+  constexpr int APP = kThreads / LPA;         // atoms per pass
+  const int gl = tid % LPA, slot = tid / LPA;
+  step_mark(d, 24);
+  // offset of this bin in the bin-sorted order, and the number of binned atoms
+  int pre = 0, tot = 0;
+  for (int b = tid; b < nbins; b += kThreads) {
+    const int c = min(__ldcg(&counts[b]), d.bin_cap);
+    tot += c;
+    if (b < tile) pre += c;
+  }
+  float4 h = make_float4(0.0f, 0.0f, 0.0f, 0.0f), u = h;
+  if (slot < cnt) {
+    h = __ldcg((const float4*)(list + (size_t)slot * RF));
+    u = __ldcg((const float4*)(list + (size_t)slot * RF + RF - 4));
+  }
+#pragma unroll
+  for (int off = 16; off >= 1; off >>= 1) {
+    pre += __shfl_xor_sync(0xffffffffu, pre, off);
+    tot += __shfl_xor_sync(0xffffffffu, tot, off);
+  }
+  if (lane == 0) {
+    red[warp] = pre;
+    red[8 + warp] = tot;
+  }
+  __syncthreads();
+  pre = 0;
+  tot = 0;
+#pragma unroll
+  for (int w = 0; w < kThreads / 32; w++) {
+    pre += red[w];
+    tot += red[8 + w];
+  }
+  for (int j0 = 0; j0 < cnt; j0 += APP) {
     const int j = j0 + slot;
     const bool valid = j < cnt;
-    gather_atom<P, KIND>(d, valid ? __float_as_int(__ldcg(&list[(size_t)j * RF + 3])) : 0, valid, gl);
-  }
-  const int novf = __ldcg(&d.ovf_count[parity]);
-  for (int j0 = 0; j0 < novf; j0 += 32) {
-    const int j = j0 + slot;
-    int atom = 0;
-    bool mine = false;
-    if (j < novf) {
-      const float4 h = __ldcg((const float4*)(d.ovf_recs + (size_t)j * RF));
-      atom = __float_as_int(h.w);
-      mine = (__float_as_int(h.y) / d.bry + d.nby * (__float_as_int(h.z) / d.brz)) == tile;
+    float4 hn = make_float4(0.0f, 0.0f, 0.0f, 0.0f), un = hn;
+    if (j + APP < cnt) {
+      hn = __ldcg((const float4*)(list + (size_t)(j + APP) * RF));
+      un = __ldcg((const float4*)(list + (size_t)(j + APP) * RF + RF - 4));
     }
-    gather_atom<P, KIND>(d, atom, mine, gl);
+    const int atom = __float_as_int(h.w);
+    // warps whose atoms all lie beyond the bin's count skip the pass (the test is warp-uniform)
+    if (j0 + (warp * 32) / LPA < cnt)
+      gather_core<P, KIND, LPA>(d, atom, valid, gl, __float_as_int(h.x), __float_as_int(h.y), __float_as_int(h.z), u.x,
+                           u.y, u.z, u.w);
+    if (valid && gl == 0) d.perm[pre + j] = atom;
+    h = hn;
+    u = un;
+    if (j0 == 0) step_mark(d, 25);
   }
+  step_mark(d, 26);
+  const int novf = __ldcg(&d.bin_meta[kMetaOvf + parity]);
+  for (int j0 = 0; j0 < novf; j0 += APP) {
+    const int j = j0 + slot;
+    bool mine = false;
+    float4 hh = make_float4(0.0f, 0.0f, 0.0f, 0.0f), uu = hh;
+    if (j < novf) {
+      hh = __ldcg((const float4*)(d.ovf_recs + (size_t)j * RF));
+      uu = __ldcg((const float4*)(d.ovf_recs + (size_t)j * RF + RF - 4));
+      mine = (__float_as_int(hh.y) / d.bry + d.nby * (__float_as_int(hh.z) / d.brz)) == tile;
+      if (tile == 0 && gl == 0) d.perm[tot + j] = __float_as_int(hh.w);
+    }
+    if (j0 + (warp * 32) / LPA < novf)
+      gather_core<P, KIND, LPA>(d, __float_as_int(hh.w), mine, gl, __float_as_int(hh.x), __float_as_int(hh.y),
+                           __float_as_int(hh.z), uu.x, uu.y, uu.z, uu.w);
+  }
+  // binned + overflow atoms are all natom atoms: the order is a permutation for this atom count
+  if (tile == 0 && tid == 0) d.bin_meta[kMetaPermNatom] = d.natom;
 }
 
 template <int P>
@@ -1093,19 +1286,29 @@ __device__ __forceinline__ void gather_dispatch(const SysDesc& d, int tile) {
 }
 
 template <int P>
-__device__ __forceinline__ void gather_bin_any(const SysDesc& d, int tile, int parity) {
-  switch (d.force_kind) {
-    case kForceF32Soa: gather_bin_tile<P, kForceF32Soa>(d, tile, parity); break;
-    case kForceF32x3: gather_bin_tile<P, kForceF32x3>(d, tile, parity); break;
-    default: gather_bin_tile<P, kForceI64SoaAccum>(d, tile, parity); break;
+__device__ __forceinline__ void gather_bin_any(const SysDesc& d, int tile, int parity, int* red, bool wide) {
+  if (wide) {
+    switch (d.force_kind) {
+      case kForceF32Soa: gather_bin_tile<P, kForceF32Soa, gather_lanes(P)>(d, tile, parity, red); break;
+      case kForceF32x3: gather_bin_tile<P, kForceF32x3, gather_lanes(P)>(d, tile, parity, red); break;
+      default: gather_bin_tile<P, kForceI64SoaAccum, gather_lanes(P)>(d, tile, parity, red); break;
+    }
+  } else {
+    switch (d.force_kind) {
+      case kForceF32Soa: gather_bin_tile<P, kForceF32Soa, 8>(d, tile, parity, red); break;
+      case kForceF32x3: gather_bin_tile<P, kForceF32x3, 8>(d, tile, parity, red); break;
+      default: gather_bin_tile<P, kForceI64SoaAccum, 8>(d, tile, parity, red); break;
+    }
   }
 }
 
-__device__ __forceinline__ void gather_bin_dispatch(const SysDesc& d, int tile, int parity) {
+// wide: gather_lanes(P) lanes per atom (few passes per bin: for launches with about one gather
+// tile per CTA); otherwise 8 (fewer partly-filled warps: for launches with many tiles per CTA).
+__device__ __forceinline__ void gather_bin_dispatch(const SysDesc& d, int tile, int parity, char* smem, bool wide) {
   switch (d.order) {
-    case 4: gather_bin_any<4>(d, tile, parity); break;
-    case 6: gather_bin_any<6>(d, tile, parity); break;
-    default: gather_bin_any<8>(d, tile, parity); break;
+    case 4: gather_bin_any<4>(d, tile, parity, (int*)smem, wide); break;
+    case 6: gather_bin_any<6>(d, tile, parity, (int*)smem, wide); break;
+    default: gather_bin_any<8>(d, tile, parity, (int*)smem, wide); break;
   }
 }
 

@@ -39,6 +39,14 @@ def _sys(name):
     if name == "long_z":      # nz > 256: the fused path runs separate y / z passes, not plane tiles
         box = (15.0, 16.0, 300.0)
         return S.PmeSystem("lz", S.water_box(1500, box, 34), box, (16, 18, 320), 4, 0.35)
+    if name == "bigq":        # two charges of +-700: the fused tile leaves its 2-sum accumulation form
+        s = _sys("odd_grid")
+        x = s.xyzq.copy()
+        x[0, 3], x[1, 3] = 700.0, -700.0
+        return S.PmeSystem("bigq", x, s.box, s.nfft, s.order, s.kappa)
+    if name == "dense_p8":    # > 65,536 candidate atoms per row block: the carry accumulation form
+        box = (20.0, 20.0, 20.0)
+        return S.PmeSystem("dense", S.water_box(45000, box, 35), box, (16, 16, 16), 8, 0.4)
     if name == "ragged33":
         box = (15.0, 15.0, 15.0)
         x = S.water_box(11, box, 33)
@@ -47,7 +55,7 @@ def _sys(name):
 
 
 CASES = ["water1k_32", "water8k_64_p4", "water8k_64_p6", "water1k_p8", "odd_grid", "noncubic_p6",
-         "one_atom", "ragged33", "long_z"]
+         "one_atom", "ragged33", "long_z", "bigq"]
 
 
 def _pme(cuda, s):
@@ -140,9 +148,13 @@ def test_reference_fixture(cuda, ref_fixture, order):
 
 
 @pytest.mark.parametrize("name,schedule", [("water8k_64_p4", 1), ("water8k_64_p4", 2),
-                                           ("long_z", 0), ("noncubic_p6", 1)])
+                                           ("long_z", 0), ("noncubic_p6", 1), ("bigq", 0),
+                                           ("dense_p8", 0)])
 def test_staged_calls_equal_fused_eval(cuda, name, schedule):
-    """Staged reference-style calls and the fused kernel (either y/z schedule) agree bit for bit."""
+    """Staged reference-style calls and the fused kernel (either y/z schedule) agree bit for bit.
+    The fused tile accumulates its charge rows in one of three exact forms, chosen from the tile's
+    candidate count and the largest |q|; water boxes take the 2-sum form, bigq the 3-sum form and
+    dense_p8 the carry form, and all must give the staged path's int64 grid."""
     s = _sys(name)
     a = _run(cuda, s, staged=True)
     pme = _pme(cuda, s)
@@ -258,3 +270,17 @@ def test_nonfinite_coordinates_stay_in_bounds(cuda, oracle):
     xd = cuda.from_numpy(x).cuda()
     pme.spread_charge(xd, bad.natom, recip_from_box(bad.box))
     assert np.array_equal(pme.charge_grid_fixed(), oracle.spread_fixed(x, bad.recip3, bad.nfft, bad.order))
+
+
+def test_atom_count_change_on_one_handle(cuda):
+    """The fused path walks atoms in the previous evaluation's bin-sorted order only when that
+    order was built for the same atom count: evaluations whose count changes on one handle equal
+    those of fresh handles bit for bit."""
+    s = _sys("water8k_64_p4")
+    fewer = S.PmeSystem("fewer", s.xyzq[:20011].copy(), s.box, s.nfft, s.order, s.kappa)
+    pme = _pme(cuda, s)
+    for sys_ in (s, fewer, fewer, s, s):
+        got = _run(cuda, sys_, pme=pme)
+        want = _run(cuda, sys_)
+        assert np.array_equal(got["force"], want["force"]), sys_.name
+        assert got["energy"] == want["energy"] and np.array_equal(got["virial"], want["virial"])
