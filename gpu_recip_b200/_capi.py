@@ -71,6 +71,11 @@ SIGNATURES = {
     "pme_set_trace": [_P, _P, _I],
     "pme_spread_charge_noalloc": [_P, _I, _DP, _I, _I, _I, _I, _P, _P],
     "pme_batch_set_trace": [_P, _P, _I],
+    "pme_autotune": [_P, _P, _I, _D, _D, _D, _D, _I, _P],
+    "pme_get_tune_config": [_P, _P],
+    "pme_set_tune_config": [_P, _P],
+    "pme_tune_cache_clear": [],
+    "pme_batch_autotune": [_P, _I, _P],
     "pme_last_error_string": [],
     "pme_status_string": [_I],
     "pme_version": [],
@@ -88,6 +93,16 @@ class SystemDesc(ctypes.Structure):
                 ("box", ctypes.c_double * 3), ("kappa", ctypes.c_double), ("xyzq", _P),
                 ("force", _P), ("force_kind", _I), ("stride", _I), ("calc_energy", _I),
                 ("calc_virial", _I)]
+
+
+class TuneConfig(ctypes.Structure):
+    """pme_tune_config of include/pme_recip.h."""
+    _fields_ = [("schedule", _I), ("x_lines", _I), ("y_lines", _I), ("z_columns", _I),
+                ("grid_ctas", _I), ("us_per_eval", ctypes.c_float), ("candidates", _I)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
 
 _lib = None
 

@@ -13,7 +13,10 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <new>
+#include <tuple>
 #include <string>
 #include <vector>
 
@@ -340,6 +343,7 @@ struct pme_recip {
   unsigned long long* trace = nullptr;
   int trace_ctas = 0;
   int plane_mode = 0;   // 0 automatic, 1 whole-plane tiles where they fit, 2 separate passes
+  int grid_cap = 0;     // CTAs of the persistent launch (0: as many as are resident)
 };
 
 struct pme_batch {
@@ -359,6 +363,8 @@ struct pme_batch {
   size_t bytes = 0;
   unsigned long long* trace = nullptr;
   int trace_ctas = 0;
+  int plane_mode = 0;   // PME_SCHED_*: AUTO and PLANES use planes where they fit
+  int grid_cap = 0;
 };
 
 namespace {
@@ -435,9 +441,54 @@ int launch_fused_single(pme_recip* h, const SysDesc& d_in) {
   int most = 1;
   for (int p = 0; p < kPhases; p++) most = std::max(most, a.total[p]);
   grid = std::max(1, std::min(grid, most));
+  if (h->grid_cap > 0) grid = std::min(grid, h->grid_cap);
   e = fused_launch(a, grid, smem, h->stream);
   if (e != cudaSuccess) return cuda_fail(e, "fused eval launch");
   return PME_OK;
+}
+
+// ---- launch shapes (autotuner) ----
+struct TuneKey {
+  int dev, nx, ny, nz, order;
+  bool operator<(const TuneKey& o) const {
+    return std::tie(dev, nx, ny, nz, order) < std::tie(o.dev, o.nx, o.ny, o.nz, o.order);
+  }
+};
+std::mutex g_tune_mutex;
+std::map<TuneKey, pme_tune_config> g_tune_cache;
+
+TuneKey tune_key(const pme_recip* h) { return TuneKey{h->device, h->st.nx, h->st.ny, h->st.nz, h->st.order}; }
+
+void get_config(const pme_recip* h, pme_tune_config* c) {
+  std::memset(c, 0, sizeof(*c));
+  c->schedule = h->plane_mode;
+  c->x_lines = h->st.tx_rows;
+  c->y_lines = h->st.tx_y;
+  c->z_columns = h->st.tx_z;
+  c->grid_ctas = h->grid_cap;
+}
+
+// Does a shape fit the fused kernel's per-tile shared-memory budget?
+bool config_fits(const SystemState& st, const pme_tune_config& c) {
+  if (c.schedule < PME_SCHED_AUTO || c.schedule > PME_SCHED_PASSES) return false;
+  if (c.x_lines < 1 || c.y_lines < 1 || c.z_columns < 1 || c.grid_ctas < 0) return false;
+  if (c.x_lines > 64 || c.y_lines > 64 || c.z_columns > 64) return false;
+  return tile_smem_bytes(st.nx, c.x_lines) <= kTileSmemBudget && tile_smem_bytes(st.ny, c.y_lines) <= kTileSmemBudget &&
+         tile_smem_bytes(st.nz, c.z_columns) + ktab_smem_bytes(st.ny, st.nz) <= kTileSmemBudget;
+}
+
+void set_config(pme_recip* h, const pme_tune_config& c) {
+  h->plane_mode = c.schedule;
+  h->st.tx_rows = c.x_lines;
+  h->st.tx_y = c.y_lines;
+  h->st.tx_z = c.z_columns;
+  h->grid_cap = c.grid_ctas;
+}
+
+void apply_cached_config(pme_recip* h) {
+  std::lock_guard<std::mutex> lock(g_tune_mutex);
+  auto it = g_tune_cache.find(tune_key(h));
+  if (it != g_tune_cache.end() && config_fits(h->st, it->second)) set_config(h, it->second);
 }
 
 }  // namespace
@@ -463,6 +514,7 @@ int pme_create(int nfftx, int nffty, int nfftz, int order, int fft_type, int nno
   e = configure_kernels(&h->max_smem);
   if (e != cudaSuccess) { delete h; return cuda_fail(e, "configure kernels"); }
   h->st.setup(nfftx, nffty, nfftz, order);
+  apply_cached_config(h);
   const size_t bytes = SystemState::bytes(nfftx, nffty, nfftz);
   if (cudaMalloc(&h->d_block, bytes) != cudaSuccess ||
       cudaMalloc(&h->d_bar, 4 * sizeof(unsigned long long)) != cudaSuccess) {
@@ -895,6 +947,7 @@ int pme_batch_commit(pme_batch* b) {
   std::vector<int> prefix((size_t)kPhases * (nsys + 1), 0);
   size_t smem = 0;
   for (int i = 0; i < nsys; i++) {
+    b->desc[i].plane = (b->st[i].plane && b->plane_mode != PME_SCHED_PASSES) ? 1 : 0;
     int cnt[kPhases];
     fused_tile_counts(b->desc[i], cnt);
     for (int p = 0; p < kPhases; p++)
@@ -914,6 +967,7 @@ int pme_batch_commit(pme_batch* b) {
   int most = 1;
   for (int p = 0; p < kPhases; p++) most = std::max(most, b->total[p]);
   b->grid = std::min(grid, most);
+  if (b->grid_cap > 0) b->grid = std::min(b->grid, b->grid_cap);
   return PME_OK;
 }
 
@@ -1000,6 +1054,225 @@ int pme_batch_set_trace(pme_batch* b, unsigned long long* dev_buf, int max_ctas)
 
 size_t pme_system_device_bytes(int nfftx, int nffty, int nfftz) {
   return SystemState::bytes(nfftx, nffty, nfftz);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// Autotuner: coordinate descent over the fused evaluation's launch shape, timed with CUDA events
+// on the stream the evaluations run on.  Every shape computes the same bits, so the search may
+// keep whichever is fastest on this GPU for this system.
+// ---------------------------------------------------------------------------------------------
+namespace {
+
+struct EventPair {
+  cudaEvent_t a = nullptr, b = nullptr;
+  cudaError_t init() {
+    cudaError_t e = cudaEventCreate(&a);
+    return e == cudaSuccess ? cudaEventCreate(&b) : e;
+  }
+  ~EventPair() {
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+  }
+};
+
+// Mean time (us) of `reps` back-to-back launches of `launch` after two untimed ones; fails if a
+// grid barrier of the fused kernel gave up.
+template <class F>
+int time_launches(F launch, cudaStream_t stream, const int* d_status, int reps, EventPair& ev, float* us) {
+  for (int i = 0; i < 2; i++)
+    if (int rc = launch()) return rc;
+  cudaError_t e = cudaEventRecord(ev.a, stream);
+  for (int i = 0; i < reps && e == cudaSuccess; i++)
+    if (int rc = launch()) return rc;
+  if (e == cudaSuccess) e = cudaEventRecord(ev.b, stream);
+  if (e == cudaSuccess) e = cudaEventSynchronize(ev.b);
+  float ms = 0.0f;
+  if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, ev.a, ev.b);
+  int status = 0;
+  if (e == cudaSuccess) e = cudaMemcpy(&status, d_status, sizeof(int), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_fail(e, "autotune: timing");
+  if (status != kStatusOk) return fail(PME_ETIMEOUT, "autotune: a grid barrier of the fused kernel timed out");
+  *us = ms * 1000.0f / (float)reps;
+  return PME_OK;
+}
+
+std::vector<int> line_values(int cur) {
+  std::vector<int> v = {4, 8, 16, 32};
+  if (std::find(v.begin(), v.end(), cur) == v.end()) v.push_back(cur);
+  return v;
+}
+
+int sm_count(int dev) {
+  int sms = 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1) sms = 1;
+  return sms;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pme_get_tune_config(const pme_recip* h, pme_tune_config* out) {
+  if (!h || !out) return fail(PME_EINVAL, "NULL argument");
+  get_config(h, out);
+  return PME_OK;
+}
+
+int pme_set_tune_config(pme_recip* h, const pme_tune_config* cfg) {
+  if (!h || !cfg) return fail(PME_EINVAL, "NULL argument");
+  if (!config_fits(h->st, *cfg)) return fail(PME_EINVAL, "launch shape out of range or over the shared-memory budget");
+  set_config(h, *cfg);
+  return PME_OK;
+}
+
+int pme_tune_cache_clear(void) {
+  std::lock_guard<std::mutex> lock(g_tune_mutex);
+  g_tune_cache.clear();
+  return PME_OK;
+}
+
+int pme_autotune(pme_recip* h, const void* xyzq, int ncoord, double inv_boxx, double inv_boxy, double inv_boxz,
+                 double kappa, int reps, pme_tune_config* out) {
+  if (int rc = handle_ok(h)) return rc;
+  if (ncoord < 0 || (ncoord > 0 && !xyzq)) return fail(PME_EINVAL, "bad xyzq/ncoord");
+  const double recip[9] = {inv_boxx, 0, 0, 0, inv_boxy, 0, 0, 0, inv_boxz};
+  if (int rc = check_recip(recip)) return rc;
+  if (!(kappa > 0.0) || !std::isfinite(kappa)) return fail(PME_EINVAL, "kappa must be positive");
+  if (reps < 1 || reps > 100000) return fail(PME_EINVAL, "reps must be in [1, 100000]");
+  DeviceGuard dg(h->device);
+  cudaError_t e = cudaSuccess;
+  if (h->accum_dirty) {
+    e = cudaMemsetAsync(h->st.accum, 0, h->st.G() * 8, h->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "autotune: clear grid");
+    h->accum_dirty = false;
+  }
+  if (int rc = ensure_bins(h, ncoord)) return rc;
+  // scratch force output and the energy/virial record to put back afterwards
+  const int stride = std::max(ncoord, 1);
+  float* force = nullptr;
+  if (cudaMalloc(&force, 3 * (size_t)stride * sizeof(float)) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(PME_ENOMEM, "autotune: scratch force allocation failed");
+  }
+  double saved[kEvCount];
+  e = cudaStreamSynchronize(h->stream);
+  if (e == cudaSuccess) e = cudaMemcpy(saved, h->st.ev, sizeof(saved), cudaMemcpyDeviceToHost);
+  EventPair ev;
+  if (e == cudaSuccess) e = ev.init();
+  if (e != cudaSuccess) {
+    cudaFree(force);
+    return cuda_fail(e, "autotune: setup");
+  }
+  const double r3[3] = {inv_boxx, inv_boxy, inv_boxz};
+  auto measure = [&](const pme_tune_config& c, float* us) {
+    set_config(h, c);
+    const SysDesc d = h->st.desc(r3, kappa, xyzq, ncoord, force, PME_FORCE_F32_SOA, stride, 1, 1);
+    return time_launches([&]() { return launch_fused_single(h, d); }, h->stream, h->d_status, reps, ev, us);
+  };
+  pme_tune_config best;
+  get_config(h, &best);
+  const pme_tune_config start = best;
+  float best_us = 0.0f;
+  int count = 1;
+  int rc = measure(best, &best_us);
+  const int sms = sm_count(h->device);
+  for (int sweep = 0; sweep < 2 && rc == PME_OK; sweep++) {
+    bool improved = false;
+    for (int knob = 0; knob < 5 && rc == PME_OK; knob++) {
+      std::vector<int> vals;
+      if (knob == 0) vals = h->st.plane ? std::vector<int>{PME_SCHED_PLANES, PME_SCHED_PASSES} : std::vector<int>{PME_SCHED_PASSES};
+      else if (knob == 1) vals = line_values(best.z_columns);
+      else if (knob == 2) vals = line_values(best.y_lines);
+      else if (knob == 3) vals = line_values(best.x_lines);
+      else vals = {0, sms};
+      for (int v : vals) {
+        pme_tune_config c = best;
+        int* field = knob == 0 ? &c.schedule : knob == 1 ? &c.z_columns : knob == 2 ? &c.y_lines
+                   : knob == 3 ? &c.x_lines : &c.grid_ctas;
+        if (*field == v) continue;
+        *field = v;
+        if (!config_fits(h->st, c)) continue;
+        float us = 0.0f;
+        rc = measure(c, &us);
+        if (rc) break;
+        count++;
+        if (us < 0.98f * best_us) {
+          best = c;
+          best_us = us;
+          improved = true;
+        }
+      }
+    }
+    if (!improved) break;
+  }
+  set_config(h, rc == PME_OK ? best : start);
+  e = cudaStreamSynchronize(h->stream);
+  if (e == cudaSuccess) e = cudaMemcpy(h->st.ev, saved, sizeof(saved), cudaMemcpyHostToDevice);
+  cudaFree(force);
+  if (rc) return rc;
+  if (e != cudaSuccess) return cuda_fail(e, "autotune: restore energy/virial");
+  best.us_per_eval = best_us;
+  best.candidates = count;
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    g_tune_cache[tune_key(h)] = best;
+  }
+  if (out) *out = best;
+  return PME_OK;
+}
+
+int pme_batch_autotune(pme_batch* b, int reps, pme_tune_config* out) {
+  if (!b) return fail(PME_EINVAL, "batch is NULL");
+  if (reps < 1 || reps > 100000) return fail(PME_EINVAL, "reps must be in [1, 100000]");
+  DeviceGuard dg(b->device);
+  const size_t nsys = b->st.size();
+  std::vector<double> saved(nsys * kEvCount);
+  cudaError_t e = cudaStreamSynchronize(b->stream);
+  for (size_t i = 0; i < nsys && e == cudaSuccess; i++)
+    e = cudaMemcpy(&saved[i * kEvCount], b->st[i].ev, kEvCount * sizeof(double), cudaMemcpyDeviceToHost);
+  EventPair ev;
+  if (e == cudaSuccess) e = ev.init();
+  if (e != cudaSuccess) return cuda_fail(e, "batch autotune: setup");
+  const int sms = sm_count(b->device);
+  const int start_mode = b->plane_mode, start_cap = b->grid_cap;
+  int best_mode = start_mode, best_cap = start_cap, count = 0, rc = PME_OK;
+  float best_us = 0.0f;
+  for (int mode : {PME_SCHED_AUTO, PME_SCHED_PASSES}) {
+    for (int cap : {0, sms}) {
+      b->plane_mode = mode;
+      b->grid_cap = cap;
+      if ((rc = pme_batch_commit(b))) break;
+      float us = 0.0f;
+      rc = time_launches([&]() { return pme_batch_eval(b); }, b->stream, b->d_status, reps, ev, &us);
+      if (rc) break;
+      if (count == 0 || us < 0.98f * best_us) {
+        best_us = us;
+        best_mode = mode;
+        best_cap = cap;
+      }
+      count++;
+    }
+    if (rc) break;
+  }
+  b->plane_mode = rc == PME_OK ? best_mode : start_mode;
+  b->grid_cap = rc == PME_OK ? best_cap : start_cap;
+  const int rc2 = pme_batch_commit(b);
+  e = cudaStreamSynchronize(b->stream);
+  for (size_t i = 0; i < nsys && e == cudaSuccess; i++)
+    e = cudaMemcpy(b->st[i].ev, &saved[i * kEvCount], kEvCount * sizeof(double), cudaMemcpyHostToDevice);
+  if (rc) return rc;
+  if (rc2) return rc2;
+  if (e != cudaSuccess) return cuda_fail(e, "batch autotune: restore energy/virial");
+  if (out) {
+    std::memset(out, 0, sizeof(*out));
+    out->schedule = best_mode;
+    out->grid_ctas = best_cap;
+    out->us_per_eval = best_us;
+    out->candidates = count;
+  }
+  return PME_OK;
 }
 
 }  // extern "C"

@@ -269,6 +269,27 @@ class CudaPMERecip:
         """PME_SCHED_AUTO / PME_SCHED_PLANES / PME_SCHED_PASSES (identical results)."""
         C.check(self._lib.pme_set_fft_schedule(self._h, int(schedule)), "set_fft_schedule")
 
+    def autotune(self, inv_box, xyzq, ncoord: int, kappa: float, reps: int = 10) -> dict:
+        """Measure launch shapes of the fused evaluation on this system and keep the fastest
+        (pme_autotune); returns the chosen shape and its time per evaluation."""
+        c = C.TuneConfig()
+        C.check(self._lib.pme_autotune(self._h, _xyzq_ptr(xyzq, ncoord), int(ncoord), float(inv_box[0]),
+                                       float(inv_box[1]), float(inv_box[2]), float(kappa), int(reps),
+                                       ctypes.byref(c)), "autotune")
+        return c.as_dict()
+
+    def get_tune_config(self) -> dict:
+        c = C.TuneConfig()
+        C.check(self._lib.pme_get_tune_config(self._h, ctypes.byref(c)), "get_tune_config")
+        return c.as_dict()
+
+    def set_tune_config(self, **cfg):
+        c = C.TuneConfig()
+        C.check(self._lib.pme_get_tune_config(self._h, ctypes.byref(c)), "get_tune_config")
+        for k, v in cfg.items():
+            setattr(c, k, v)
+        C.check(self._lib.pme_set_tune_config(self._h, ctypes.byref(c)), "set_tune_config")
+
     def set_fault_injection(self, what: int):
         C.check(self._lib.pme_set_fault_injection(self._h, int(what)), "set_fault_injection")
 
@@ -383,6 +404,12 @@ class PmeBatch:
         else:
             C.check(self._lib.pme_batch_set_trace(self._h, _ptr(buf), int(max_ctas or buf.numel() // 14)), "set_trace")
 
+    def autotune(self, reps: int = 5) -> dict:
+        """Measure the batch's y/z schedule and launch size and keep the fastest."""
+        c = C.TuneConfig()
+        C.check(self._lib.pme_batch_autotune(self._h, int(reps), ctypes.byref(c)), "batch autotune")
+        return c.as_dict()
+
     def info(self):
         n = ctypes.c_int()
         g = ctypes.c_int()
@@ -393,3 +420,8 @@ class PmeBatch:
 
 def system_device_bytes(nfft) -> int:
     return int(C.load().pme_system_device_bytes(int(nfft[0]), int(nfft[1]), int(nfft[2])))
+
+
+def tune_cache_clear() -> None:
+    """Forget the launch shapes pme_autotune stored for later handles of the same grid."""
+    C.check(C.load().pme_tune_cache_clear(), "tune_cache_clear")

@@ -128,6 +128,32 @@ PME_API int pme_reserve_atoms(pme_recip* h, int natom);
  * PME_SCHED_PASSES as separate y and z passes (more, smaller tiles), PME_SCHED_AUTO (default)
  * picks planes only when there are at least as many planes as SMs.  Results are identical. */
 enum { PME_SCHED_AUTO = 0, PME_SCHED_PLANES = 1, PME_SCHED_PASSES = 2 };
+
+/* ---- autotuner ----
+ * No counterpart in the reference (its launch shapes are fixed).  The fused evaluation's launch
+ * shape: the y/z schedule, the lines of the x-, y- and z-pass tiles and the number of CTAs of the
+ * persistent launch.  Every shape gives the same results bit for bit; only the time differs.
+ * pme_autotune measures candidate shapes on the caller's own system (coordinates, box, kappa as
+ * for pme_eval_ortho) by coordinate descent, `reps` timed evaluations per candidate, keeps the
+ * fastest in the handle and in a process-wide cache keyed by (device, grid, order) that later
+ * pme_create calls of the same key start from.  It synchronises the stream, allocates a
+ * temporary force buffer and leaves the energy/virial record as it found it. */
+typedef struct {
+  int schedule;        /* PME_SCHED_* */
+  int x_lines;         /* grid lines per x-pass tile */
+  int y_lines;         /* grid lines per y-pass tile */
+  int z_columns;       /* grid columns per z-pass tile */
+  int grid_ctas;       /* CTAs of the persistent launch; 0 = as many as are resident */
+  float us_per_eval;   /* measured time of this shape (pme_autotune), else 0 */
+  int candidates;      /* shapes measured (pme_autotune), else 0 */
+} pme_tune_config;
+
+PME_API int pme_autotune(pme_recip* h, const void* xyzq, int ncoord, double inv_boxx, double inv_boxy,
+                         double inv_boxz, double kappa, int reps, pme_tune_config* out);
+PME_API int pme_get_tune_config(const pme_recip* h, pme_tune_config* out);
+/* Set a shape explicitly (checked against the shared-memory limits; PME_EINVAL if it does not fit). */
+PME_API int pme_set_tune_config(pme_recip* h, const pme_tune_config* cfg);
+PME_API int pme_tune_cache_clear(void);
 PME_API int pme_set_fft_schedule(pme_recip* h, int schedule);
 
 /* Test hook for failure detection: PME_INJECT_SKIP_BARRIER makes CTA 0 of the next fused
@@ -174,6 +200,12 @@ PME_API int pme_batch_clear_energy_virial(pme_batch* b);
 PME_API int pme_batch_get_energy_virial(pme_batch* b, double* out);
 PME_API int pme_batch_info(const pme_batch* b, int* nsys, int* grid_ctas, size_t* device_bytes);
 PME_API int pme_batch_set_trace(pme_batch* b, unsigned long long* dev_buf, int max_ctas);
+/* Autotune the batch's launch: the y/z schedule of every system (planes where they fit, or
+ * passes) and the CTAs of the launch, `reps` timed evaluations per candidate; the fastest is kept
+ * (and committed).  The evaluations write the systems' force outputs as pme_batch_eval does (int64
+ * outputs accumulate every tuning evaluation: clear them afterwards); the energy/virial records are
+ * left as they were.  out may be NULL; out->x_lines, y_lines and z_columns are 0 (per system). */
+PME_API int pme_batch_autotune(pme_batch* b, int reps, pme_tune_config* out);
 /* Device bytes one system of this grid occupies (for admission by HBM footprint). */
 PME_API size_t pme_system_device_bytes(int nfftx, int nffty, int nfftz);
 
