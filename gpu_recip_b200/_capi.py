@@ -76,12 +76,18 @@ SIGNATURES = {
     "pme_set_tune_config": [_P, _P],
     "pme_tune_cache_clear": [],
     "pme_batch_autotune": [_P, _I, _P],
+    "pme_server_create": [ctypes.c_size_t, _I, _P, ctypes.POINTER(_P)],
+    "pme_server_destroy": [_P],
+    "pme_request_device_bytes": [_P],
+    "pme_server_submit": [_P, _P, ctypes.POINTER(ctypes.c_longlong)],
+    "pme_server_wait": [_P, ctypes.c_longlong, _D, _DP],
+    "pme_server_get_stats": [_P, _P],
     "pme_last_error_string": [],
     "pme_status_string": [_I],
     "pme_version": [],
 }
 _RESTYPES = {"pme_last_error_string": ctypes.c_char_p, "pme_status_string": ctypes.c_char_p,
-             "pme_system_device_bytes": ctypes.c_size_t}
+             "pme_system_device_bytes": ctypes.c_size_t, "pme_request_device_bytes": ctypes.c_size_t}
 
 PME_INJECT_NONE, PME_INJECT_SKIP_BARRIER = 0, 1
 PME_SCHED_AUTO, PME_SCHED_PLANES, PME_SCHED_PASSES = 0, 1, 2
@@ -99,6 +105,26 @@ class TuneConfig(ctypes.Structure):
     """pme_tune_config of include/pme_recip.h."""
     _fields_ = [("schedule", _I), ("x_lines", _I), ("y_lines", _I), ("z_columns", _I),
                 ("grid_ctas", _I), ("us_per_eval", ctypes.c_float), ("candidates", _I)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class Request(ctypes.Structure):
+    """pme_request of include/pme_recip.h."""
+    _fields_ = [("nfftx", _I), ("nffty", _I), ("nfftz", _I), ("order", _I), ("natom", _I),
+                ("box", ctypes.c_double * 3), ("kappa", ctypes.c_double), ("xyzq", _P),
+                ("n_evals", _I), ("sigma", ctypes.c_float), ("seed", ctypes.c_ulonglong),
+                ("calc_energy", _I), ("calc_virial", _I), ("ev_out", _P), ("force_out", _P)]
+
+
+class ServerStats(ctypes.Structure):
+    """pme_server_stats of include/pme_recip.h."""
+    _fields_ = [("submitted", ctypes.c_longlong), ("completed", ctypes.c_longlong),
+                ("evals", ctypes.c_longlong), ("steps", ctypes.c_longlong),
+                ("active", ctypes.c_longlong), ("pending", ctypes.c_longlong),
+                ("arena_bytes", ctypes.c_size_t), ("arena_used", ctypes.c_size_t),
+                ("seconds", ctypes.c_double)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -425,3 +425,80 @@ def system_device_bytes(nfft) -> int:
 def tune_cache_clear() -> None:
     """Forget the launch shapes pme_autotune stored for later handles of the same grid."""
     C.check(C.load().pme_tune_cache_clear(), "tune_cache_clear")
+
+
+class PmeServer:
+    """Request loop with continuous batching (pme_server_* of the C ABI).
+
+    submit() takes one system (a PmeSystem-like object with xyzq, box, nfft, order, kappa) and a
+    number of evaluations on its coordinates plus a seeded Gaussian jitter of sigma (A); wait()
+    returns that request's per-evaluation energy/virial records, the last evaluation's forces and
+    its submit / admission / completion times."""
+
+    def __init__(self, device_bytes: int, max_active: int = 256, stream=None):
+        self._lib = C.load()
+        h = ctypes.c_void_p()
+        C.check(self._lib.pme_server_create(int(device_bytes), int(max_active),
+                                            ctypes.c_void_p(_stream_handle(stream)), ctypes.byref(h)),
+                "pme_server_create")
+        self._h = h
+        self._live = {}
+
+    @staticmethod
+    def _request(system, n_evals, sigma, seed, ev, force, calc_energy=True, calc_virial=True):
+        x = np.ascontiguousarray(system.xyzq, dtype=np.float32)
+        r = C.Request()
+        r.nfftx, r.nffty, r.nfftz = (int(v) for v in system.nfft)
+        r.order = int(system.order)
+        r.natom = int(x.shape[0])
+        for d in range(3):
+            r.box[d] = float(system.box[d])
+        r.kappa = float(system.kappa)
+        r.xyzq = x.ctypes.data
+        r.n_evals = int(n_evals)
+        r.sigma = float(sigma)
+        r.seed = int(seed)
+        r.calc_energy, r.calc_virial = int(calc_energy), int(calc_virial)
+        r.ev_out = ev.ctypes.data
+        r.force_out = force.ctypes.data if force is not None else None
+        return r, x
+
+    @staticmethod
+    def request_device_bytes(system, n_evals: int = 1) -> int:
+        ev = np.zeros((max(int(n_evals), 1), C.PME_EV_COUNT))
+        r, _ = PmeServer._request(system, n_evals, 0.0, 0, ev, None)
+        return int(C.load().pme_request_device_bytes(ctypes.byref(r)))
+
+    def submit(self, system, n_evals: int = 1, sigma: float = 0.0, seed: int = 0, forces: bool = True) -> int:
+        ev = np.zeros((int(n_evals), C.PME_EV_COUNT), dtype=np.float64)
+        force = np.zeros((system.xyzq.shape[0], 3), dtype=np.float32) if forces else None
+        r, x = self._request(system, n_evals, sigma, seed, ev, force)
+        rid = ctypes.c_longlong()
+        C.check(self._lib.pme_server_submit(self._h, ctypes.byref(r), ctypes.byref(rid)), "server submit")
+        self._live[rid.value] = (ev, force, x)
+        return rid.value
+
+    def wait(self, rid: int, timeout: float = -1.0) -> dict:
+        t = (ctypes.c_double * 3)()
+        rc = self._lib.pme_server_wait(self._h, ctypes.c_longlong(rid), float(timeout), t)
+        ev, force, _ = self._live.pop(rid) if rc == C.PME_OK else self._live.get(rid, (None, None, None))
+        C.check(rc, "server wait")
+        return {"ev": ev, "force": force, "t_submit": t[0], "t_admit": t[1], "t_done": t[2],
+                "latency": t[2] - t[0]}
+
+    def stats(self) -> dict:
+        st = C.ServerStats()
+        C.check(self._lib.pme_server_get_stats(self._h, ctypes.byref(st)), "server stats")
+        return st.as_dict()
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self._lib.pme_server_destroy(self._h)
+            self._h = ctypes.c_void_p()
+        self._live = {}
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -209,6 +209,51 @@ PME_API int pme_batch_autotune(pme_batch* b, int reps, pme_tune_config* out);
 /* Device bytes one system of this grid occupies (for admission by HBM footprint). */
 PME_API size_t pme_system_device_bytes(int nfftx, int nffty, int nfftz);
 
+/* ---- request server: continuous batching of PME evaluations ----
+ * No counterpart in the reference, whose CudaDomdecRecipLooper (CudaDomdecRecipLooper.cu:3-36)
+ * serves one system's evaluations at a time.  A server owns a device arena of device_bytes and a
+ * worker thread.  A request is one orthorhombic system and n_evals evaluations of it; evaluation k
+ * uses the submitted coordinates plus sigma * N(0,1) per coordinate, drawn from (seed, k, atom,
+ * axis), so a request's results depend only on the request.  Requests are admitted in arrival
+ * order while fewer than max_active run and their device footprint (pme_request_device_bytes)
+ * fits in the arena; every step evaluates the next evaluation of all running requests in one
+ * fused launch; requests that arrive meanwhile join at the next step.  A request's grids, moduli,
+ * bins and bin-sorted atom order stay on the device for all its evaluations. */
+typedef struct pme_server pme_server;
+typedef struct {
+  int nfftx, nffty, nfftz, order;
+  int natom;
+  double box[3];            /* orthorhombic box edges (A) */
+  double kappa;
+  const float* xyzq;        /* host float[natom][4]; copied by pme_server_submit */
+  int n_evals;              /* >= 1 */
+  float sigma;              /* coordinate jitter (A) of every evaluation; 0 = none */
+  unsigned long long seed;
+  int calc_energy, calc_virial;
+  double* ev_out;           /* host n_evals * PME_EV_COUNT doubles: each evaluation's record */
+  float* force_out;         /* host natom * 3 floats (x, y, z per atom) of the last evaluation, or NULL */
+} pme_request;
+
+typedef struct {
+  long long submitted, completed, evals, steps, active, pending;
+  size_t arena_bytes, arena_used;
+  double seconds;           /* since the server was created */
+} pme_server_stats;
+
+/* stream NULL: the server makes its own non-blocking stream. */
+PME_API int pme_server_create(size_t device_bytes, int max_active, void* stream, pme_server** out);
+/* Finishes every admitted and pending request, then releases everything. */
+PME_API int pme_server_destroy(pme_server* s);
+PME_API size_t pme_request_device_bytes(const pme_request* r);   /* 0 if the request is invalid */
+/* Queue a request (PME_ENOMEM if it can never fit in the arena); the host buffers ev_out and
+ * force_out must stay valid until pme_server_wait for its id returns. */
+PME_API int pme_server_submit(pme_server* s, const pme_request* r, long long* id);
+/* Block until request `id` is done (timeout_s < 0: no limit); its results are then in ev_out /
+ * force_out; times3 (may be NULL) receives its submit, admission and completion times (seconds
+ * since the server was created).  Each id can be waited for once. */
+PME_API int pme_server_wait(pme_server* s, long long id, double timeout_s, double* times3);
+PME_API int pme_server_get_stats(pme_server* s, pme_server_stats* out);
+
 /* ---- spreading without device allocation ----
  * No counterpart in the reference.  For callers that must not allocate device memory when they
  * need a charge grid: code running while a stream is captured into a CUDA graph, hosts whose own
