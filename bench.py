@@ -33,9 +33,9 @@ sys.path.insert(0, ROOT)
 
 METRIC = "PME recip evals/s at 24k atoms/64^3; batched evals/s + p50/p99 latency, same GPU"
 
-# DRAM bytes (read + write) of one k_fused launch from an ncu capture, by workload (None until
-# captured).  Filled from profiles/ summaries.
-TRAFFIC_BYTES = {}
+# DRAM bytes (read + write) of one k_fused launch from an ncu capture, by workload (mean of 3
+# launches; profiles/k_fused_water8k_64_p4_full.md).  None where not captured.
+TRAFFIC_BYTES = {"water8k_64_p4": 700160}
 UNIT = "evals/s"
 FALLBACK_HBM_GBS = 6650.0
 
@@ -52,6 +52,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch", type=int, default=256, help="systems in the batched measurement (0: skip)")
     ap.add_argument("--batch-steps", type=int, default=200)
+    ap.add_argument("--serve-requests", type=int, default=600, help="requests of the serving run (0: skip)")
+    ap.add_argument("--serve-rate", type=float, default=400.0, help="Poisson arrival rate (requests/s)")
     return ap.parse_args()
 
 
@@ -197,25 +199,17 @@ def run_reference(args):
 
 def run_b200(args):
     import torch
-    import torch.distributed as dist
-
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        from datetime import timedelta
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
-    else:
-        torch.cuda.set_device(0)
+    from gpu_recip_b200 import replicas as R
+    rank, world, local = R.rank_world()
+    torch.cuda.set_device(local if world > 1 else 0)
+    R.init("nccl")
     dev = torch.device("cuda", torch.cuda.current_device())
 
     from gpu_recip_b200 import CudaPMERecip, force_stride, load_library
     from gpu_recip_b200 import build as B
     if rank == 0 or world == 1:
         B.build()
-    if world > 1:
-        dist.barrier()
+    R.barrier()
     load_library()
 
     s = make_workload(args.workload, rank)
@@ -240,13 +234,19 @@ def run_b200(args):
             flush.fill_(0.0)
             one_eval()
     stream.synchronize()
+    # launch shape of the fused kernel from the autotuner (results are the same for every shape)
+    tune = pme.autotune(inv_box, x_dev, n, s.kappa, reps=10)
+    with torch.cuda.stream(stream):
+        for _ in range(3):
+            flush.fill_(0.0)
+            one_eval()
+    stream.synchronize()
 
     K = args.steps
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
     clocks = ClockSampler(dev.index)
-    if world > 1:
-        dist.barrier()
+    R.barrier()
     torch.cuda.synchronize()
     with clocks:
         with torch.cuda.stream(stream):
@@ -258,13 +258,9 @@ def run_b200(args):
         stream.synchronize()
     torch.cuda.synchronize()
     per = np.array([starts[i].elapsed_time(ends[i]) for i in range(K)])  # ms
-    total_ms = float(per.sum())
-    if world > 1:
-        t = torch.tensor([total_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-        dist.barrier()
-    value = world * K / (total_ms / 1000.0)
+    total_ms = R.max_over_ranks(float(per.sum()), dev)      # slowest replica
+    R.barrier()
+    value = R.aggregate_rate([K] * world, total_ms / 1000.0)
 
     # ---- e2e through the C ABI with host buffers -------------------------------------------------
     x_host = torch.from_numpy(s.xyzq).pin_memory()
@@ -287,12 +283,8 @@ def run_b200(args):
             if i >= 3:
                 e_ends[i - 3].record(stream)
     stream.synchronize()
-    e_total = float(sum(e_starts[i].elapsed_time(e_ends[i]) for i in range(Ke)))
-    if world > 1:
-        t = torch.tensor([e_total], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e_total = float(t.item())
-    e2e_value = world * Ke / (e_total / 1000.0)
+    e_total = R.max_over_ranks(float(sum(e_starts[i].elapsed_time(e_ends[i]) for i in range(Ke))), dev)
+    e2e_value = R.aggregate_rate([Ke] * world, e_total / 1000.0)
 
     # ---- staged C-ABI calls, per reference stage (informational) -----------------------------------
     stages = stage_times(pme, s, x_dev, f_dev, stride, recip, stream, flush)
@@ -307,10 +299,17 @@ def run_b200(args):
                 "alg_bytes_per_launch": s.alg_bytes(),
                 "staged_stage_us": {k: v * 1000 for k, v in stages.items()}}
 
+    fft_cmp = fft_comparator(s, stages, dev)
+
     # ---- batched: uneven systems in one persistent launch --------------------------------------------
     batched = None
     if args.batch > 0:
         batched = run_batched(args, dev, stream, flush, rank, world)
+
+    # ---- serving: Poisson request stream, continuous batching vs the plain path ------------------
+    serving = None
+    if args.serve_requests > 0:
+        serving = run_serving(args, dev, rank, world)
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -323,27 +322,29 @@ def run_b200(args):
                 "warmup": args.warmup, "ms_per_step": total_ms / K, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32+i64 fixed-point grid",
                 "data": "synthetic (seeded TIP3P-geometry water)",
-                "config": workload_config(s, {"parallelism": f"replicas x{world}" if world > 1 else "single GPU"}),
+                "config": workload_config(s, {"parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                                              "launch_shape": {k: tune[k] for k in ("schedule", "x_lines", "y_lines",
+                                                                                     "z_columns", "grid_ctas")}}),
                 "latency_ms": {"p50": float(np.percentile(per, 50)), "p99": float(np.percentile(per, 99))},
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 16 * n,
                         "d2h_bytes_per_step": 4 * 3 * stride + 8 * 11},
                 "gpu_launches": kernels_per_eval * K,
-                "roofline": roofline, "batched": batched,
+                "roofline": roofline, "batched": batched, "serving": serving, "fft_comparator": fft_cmp,
                 "clocks": clocks.summary(), "cpu_baseline": cpu}
         print(json.dumps(line), flush=True)
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
+    R.barrier()
+    R.shutdown()
 
 
 def run_batched(args, dev, stream, flush, rank, world):
     """256 independent water boxes of 648-24,000 atoms, 24^3-64^3 grids, order 4, kappa 0.32, all
-    evaluated by one persistent launch per step (L2 flushed before every step)."""
+    evaluated by one persistent launch per step, launch shape picked by the batch autotuner and the
+    step replayed from a CUDA graph (L2 flushed before every step, outside the timed events)."""
     import torch
-    import torch.distributed as dist
     from gpu_recip_b200 import PmeBatch, force_stride
+    from gpu_recip_b200 import replicas as R
     from gpu_recip_b200 import systems as S
-    systems = S.batch_systems(args.batch, seed=4 + 1000 * rank)
+    systems = S.batch_systems(args.batch, seed=R.replica_seed(4, rank))
     specs = []
     for sy in systems:
         x = torch.from_numpy(sy.xyzq).to(dev)
@@ -351,42 +352,161 @@ def run_batched(args, dev, stream, flush, rank, world):
         f = torch.zeros(3 * st, dtype=torch.float32, device=dev)
         specs.append(dict(nfft=sy.nfft, order=sy.order, box=sy.box, kappa=sy.kappa, xyzq=x, force=f, stride=st))
     b = PmeBatch(specs, stream=stream)
+    tune = b.autotune(reps=5)
     with torch.cuda.stream(stream):
         for _ in range(3):
             flush.fill_(0.0)
             b.clear_energy_virial()
             b.eval()
     stream.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=stream):
+        b.clear_energy_virial()
+        b.eval()
     K = args.batch_steps
     st_ev = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
     en_ev = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
-    if world > 1:
-        dist.barrier()
+    R.barrier()
     torch.cuda.synchronize()
     with torch.cuda.stream(stream):
         for i in range(K):
             flush.fill_(float(i & 7))
             st_ev[i].record(stream)
-            b.clear_energy_virial()
-            b.eval()
+            graph.replay()
             en_ev[i].record(stream)
     stream.synchronize()
     per = np.array([st_ev[i].elapsed_time(en_ev[i]) for i in range(K)])
-    total = float(per.sum())
-    if world > 1:
-        t = torch.tensor([total], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total = float(t.item())
+    total = R.max_over_ranks(float(per.sum()), dev)
+    del graph
     peak, _ = measured_peak()
     alg = sum(sy.alg_bytes() for sy in systems)
     ms = total / K
     info = b.info()
     return {"systems": len(systems), "atoms": int(sum(sy.natom for sy in systems)),
-            "evals_per_s": world * len(systems) * K / (total / 1000.0), "ms_per_batch": ms,
+            "evals_per_s": R.aggregate_rate([len(systems) * K] * world, total / 1000.0), "ms_per_batch": ms,
             "p50_ms": float(np.percentile(per, 50)), "p99_ms": float(np.percentile(per, 99)),
-            "launches_per_batch": 1, "grid_ctas": info["grid_ctas"],
+            "launches_per_batch": 1, "cuda_graph": True, "grid_ctas": info["grid_ctas"],
+            "autotune": {"schedule": ["auto", "planes", "passes"][tune["schedule"]], "grid_ctas": tune["grid_ctas"],
+                         "candidates": tune["candidates"]},
             "device_bytes": info["device_bytes"], "alg_bytes_per_batch": alg,
             "roofline_frac": alg / (ms * 1e-3) / 1e9 / peak}
+
+
+def serving_stream(n: int, rate: float, seed: int):
+    """Poisson arrivals (s), system indices into a pool of batch-distribution systems, evaluation
+    counts 1-100 and jitter seeds."""
+    rng = np.random.default_rng(seed)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=n)) if rate > 0 else np.zeros(n)
+    return arrivals, rng.integers(0, 64, size=n), rng.integers(1, 101, size=n), rng.integers(1, 2 ** 62, size=n)
+
+
+def run_serving(args, dev, rank, world):
+    """Requests drawn from the batch distribution (648-24,000 atoms, 24^3-64^3 grids), 1-100
+    evaluations each with 0.05 A Gaussian coordinate jitter, arriving as a Poisson stream: the
+    continuous-batching server against the plain single-system path (one request at a time,
+    first come first served, one cached handle per grid) on the same stream.  Latency = completion
+    - arrival; evals/s = all evaluations / (last completion - first arrival).  Also the server's
+    throughput with every request queued at once."""
+    import threading
+    import torch
+    from gpu_recip_b200 import CudaPMERecip, PmeServer
+    from gpu_recip_b200 import replicas as R
+    from gpu_recip_b200 import systems as S
+    pool = S.batch_systems(64, seed=R.replica_seed(11, rank))
+    n = args.serve_requests
+    arrivals, idx, nev, seeds = serving_stream(n, args.serve_rate, R.replica_seed(23, rank))
+    sigma = 0.05
+
+    def serve(rate_arrivals):
+        srv = PmeServer(24 << 30, max_active=256)
+        srv.wait(srv.submit(pool[0], n_evals=2, sigma=sigma, seed=1))       # warm-up
+        ids = [None] * n
+        t0 = time.perf_counter()
+
+        def submitter():
+            for i in range(n):
+                dt = t0 + rate_arrivals[i] - time.perf_counter()
+                if dt > 0:
+                    time.sleep(dt)
+                ids[i] = srv.submit(pool[idx[i]], n_evals=int(nev[i]), sigma=sigma, seed=int(seeds[i]))
+
+        th = threading.Thread(target=submitter)
+        th.start()
+        th.join()
+        res = [srv.wait(rid, timeout=600) for rid in ids]
+        st = srv.stats()
+        srv.close()
+        lat = np.array([r["latency"] for r in res]) * 1000.0
+        span = max(r["t_done"] for r in res) - min(r["t_submit"] for r in res)
+        return {"evals_per_s": float(nev.sum()) / span, "p50_ms": float(np.percentile(lat, 50)),
+                "p99_ms": float(np.percentile(lat, 99)), "steps": st["steps"], "seconds": span}
+
+    served = serve(arrivals)
+    saturated = serve(np.zeros(n))
+
+    # plain path: one request at a time in arrival order
+    handles = {}
+    xs = [torch.from_numpy(sy.xyzq).to(dev) for sy in pool]
+    gen = torch.Generator(device=dev)
+    lat = []
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for i in range(n):
+        wait = t0 + arrivals[i] - time.perf_counter()
+        if wait > 0:
+            time.sleep(wait)
+        sy = pool[idx[i]]
+        key = (tuple(sy.nfft), sy.order)
+        if key not in handles:
+            handles[key] = CudaPMERecip(*sy.nfft, sy.order)
+        pme = handles[key]
+        gen.manual_seed(int(seeds[i]) & 0x7FFFFFFF)
+        f = torch.empty((sy.natom, 3), dtype=torch.float32, device=dev)
+        ev = np.zeros((int(nev[i]), 11))
+        for k in range(int(nev[i])):
+            x = xs[idx[i]].clone()
+            x[:, :3] += sigma * torch.randn((sy.natom, 3), generator=gen, device=dev)
+            pme.energy_virial.clear()
+            pme.eval_ortho([1.0 / b for b in sy.box], x, sy.natom, sy.kappa, True, True, f, 1)
+            pme.energy_virial.copyToHost()
+            ev[k, 0] = pme.energy_virial.getEnergy("recip")
+        f.cpu()
+        lat.append((time.perf_counter() - t0 - arrivals[i]) * 1000.0)
+    span = time.perf_counter() - t0
+    plain = {"evals_per_s": float(nev.sum()) / span, "p50_ms": float(np.percentile(lat, 50)),
+             "p99_ms": float(np.percentile(lat, 99)), "seconds": span}
+    total = R.sum_over_ranks(float(nev.sum()), dev)
+    return {"requests": n, "rate_per_s": args.serve_rate, "evals": int(nev.sum()), "sigma_A": sigma,
+            "pool_systems": len(pool), "evals_per_request": "uniform 1-100",
+            "server": served, "server_all_queued": saturated, "plain_path": plain,
+            "all_ranks_evals": total}
+
+
+def fft_comparator(s, stages, dev):
+    """cuFFT (torch.fft) 3-D R2C + C2R of the workload's grid, timed like the staged calls, beside
+    this engine's staged r2c_fft + c2r_fft (each of which also converts the fixed-point grid or
+    writes the real grid).  Timing only: cuFFT is never on the product path."""
+    import torch
+    nx, ny, nz = s.nfft
+    g = torch.randn((nz, ny, nx), dtype=torch.float32, device=dev)
+    for _ in range(5):
+        torch.fft.irfftn(torch.fft.rfftn(g), s=(nz, ny, nx))
+    torch.cuda.synchronize()
+    reps = 50
+    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    fwd = inv = 0.0
+    for _ in range(reps):
+        e0.record()
+        h = torch.fft.rfftn(g)
+        e1.record()
+        torch.fft.irfftn(h, s=(nz, ny, nx))
+        e2.record()
+        torch.cuda.synchronize()
+        fwd += e0.elapsed_time(e1)
+        inv += e1.elapsed_time(e2)
+    return {"cufft_r2c_us": 1000 * fwd / reps, "cufft_c2r_us": 1000 * inv / reps,
+            "b200_r2c_fft_us": 1000 * stages["r2c_fft"], "b200_c2r_fft_us": 1000 * stages["c2r_fft"],
+            "note": "cuFFT timed as a comparator only (torch.fft); L2 warm for both"}
 
 
 def stage_times(pme, s, x, f, stride, recip, stream, flush, reps: int = 50):
