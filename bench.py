@@ -52,6 +52,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch", type=int, default=256, help="systems in the batched measurement (0: skip)")
     ap.add_argument("--batch-steps", type=int, default=200)
+    ap.add_argument("--large-steps", type=int, default=20, help="timed evaluations of the 216^3 system (0: skip)")
     ap.add_argument("--serve-requests", type=int, default=600, help="requests of the serving run (0: skip)")
     ap.add_argument("--serve-rate", type=float, default=400.0, help="Poisson arrival rate (requests/s)")
     return ap.parse_args()
@@ -306,6 +307,11 @@ def run_b200(args):
     if args.batch > 0:
         batched = run_batched(args, dev, stream, flush, rank, world)
 
+    # ---- large system: 1,008,000 atoms, 216^3, order 6 -------------------------------------------
+    large = None
+    if args.large_steps > 0:
+        large = run_large(args, dev, stream, flush, rank, world)
+
     # ---- serving: Poisson request stream, continuous batching vs the plain path ------------------
     serving = None
     if args.serve_requests > 0:
@@ -329,7 +335,8 @@ def run_b200(args):
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 16 * n,
                         "d2h_bytes_per_step": 4 * 3 * stride + 8 * 11},
                 "gpu_launches": kernels_per_eval * K,
-                "roofline": roofline, "batched": batched, "serving": serving, "fft_comparator": fft_cmp,
+                "roofline": roofline, "batched": batched, "serving": serving, "large": large,
+                "fft_comparator": fft_cmp,
                 "clocks": clocks.summary(), "cpu_baseline": cpu}
         print(json.dumps(line), flush=True)
     R.barrier()
@@ -390,6 +397,61 @@ def run_batched(args, dev, stream, flush, rank, world):
                          "candidates": tune["candidates"]},
             "device_bytes": info["device_bytes"], "alg_bytes_per_batch": alg,
             "roofline_frac": alg / (ms * 1e-3) / 1e9 / peak}
+
+
+def stage_alg_bytes(s):
+    """Algorithmic bytes of each staged call: each stage reads its input and writes its output
+    once (FP32 real grid, FP32 complex)."""
+    N, (nx, ny, nz) = s.natom, s.nfft
+    G, H = nx * ny * nz, (nx // 2 + 1) * ny * nz
+    return {"spread": 16 * N + 4 * G, "r2c_fft": 4 * G + 8 * H, "scalar_sum": 16 * H,
+            "c2r_fft": 8 * H + 4 * G, "gather": 28 * N + 4 * G, "self_energy": 16 * N}
+
+
+def run_large(args, dev, stream, flush, rank, world):
+    """The 216^3 configuration (1,008,000 atoms, order 6, kappa 0.30): fused evaluations with L2
+    flushed between steps, plus each staged stage against its algorithmic bytes."""
+    import torch
+    from gpu_recip_b200 import CudaPMERecip, force_stride
+    from gpu_recip_b200 import replicas as R
+    from gpu_recip_b200 import systems as S
+    s = S.config_large(seed=R.replica_seed(3, rank))
+    n = s.natom
+    st = force_stride(n)
+    pme = CudaPMERecip(*s.nfft, s.order, stream=stream)
+    inv_box = [1.0 / b for b in s.box]
+    recip = [inv_box[0], 0, 0, 0, inv_box[1], 0, 0, 0, inv_box[2]]
+    x = torch.from_numpy(s.xyzq).to(dev)
+    f = torch.zeros(3 * st, dtype=torch.float32, device=dev)
+    tune = pme.autotune(inv_box, x, n, s.kappa, reps=3)
+    K = args.large_steps
+    ev0 = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    ev1 = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    with torch.cuda.stream(stream):
+        for i in range(K + 2):
+            flush.fill_(float(i & 7))
+            if i >= 2:
+                ev0[i - 2].record(stream)
+            pme.energy_virial.clear()
+            pme.eval_ortho(inv_box, x, n, s.kappa, True, True, f, st)
+            if i >= 2:
+                ev1[i - 2].record(stream)
+    stream.synchronize()
+    total = R.max_over_ranks(float(sum(ev0[i].elapsed_time(ev1[i]) for i in range(K))), dev)
+    ms = total / K
+    peak, _ = measured_peak()
+    stages = stage_times(pme, s, x, f, st, recip, stream, flush, reps=5)
+    alg = stage_alg_bytes(s)
+    per_stage = {k: {"us": 1000 * stages[k], "alg_bytes": alg[k],
+                     "GBps": alg[k] / (stages[k] * 1e-3) / 1e9,
+                     "roofline_frac": alg[k] / (stages[k] * 1e-3) / 1e9 / peak} for k in stages}
+    return {"workload": f"{s.name}: {n} atoms, box {s.box[0]:.1f} A, grid {s.nfft[0]}^3, order {s.order}, "
+                        f"kappa {s.kappa}", "steps": K, "ms_per_eval": ms,
+            "evals_per_s": R.aggregate_rate([K] * world, total / 1000.0),
+            "alg_bytes_per_eval": s.alg_bytes(),
+            "roofline_frac": s.alg_bytes() / (ms * 1e-3) / 1e9 / peak,
+            "launch_shape": {k: tune[k] for k in ("schedule", "x_lines", "y_lines", "z_columns", "grid_ctas")},
+            "staged_stages": per_stage}
 
 
 def serving_stream(n: int, rate: float, seed: int):
