@@ -194,7 +194,9 @@ struct SystemState {
     // row blocks of the fused spread + x pass: the largest square block that fits
     for (int b = kSpreadMaxBlock; b >= 1; b--) {
       bry = brz = b;
-      if (spread_x_smem_bytes(nx, b * b, kMaxOrder) <= kTileSmemBudget) break;
+      size_t need = 0;   // the order can change later (pme_set_order): size for every order
+      for (int o = 4; o <= kMaxOrder; o += 2) need = std::max(need, spread_x_smem_bytes(nx, b * b, o));
+      if (need <= kTileSmemBudget) break;
     }
     nby = (ny + bry - 1) / bry;
     nbz = (nz + brz - 1) / brz;

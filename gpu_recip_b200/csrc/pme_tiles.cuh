@@ -669,27 +669,31 @@ __device__ __forceinline__ void bin_tile(const SysDesc& d, int tile, int parity,
 // the result equals the staged spread's fixed-point grid bit for bit), then the rows are converted
 // to FP32 and x-transformed in place.
 //
-// The work is split so that every lane does the same amount: a round takes up to kSpreadSlots
-// candidates; step A tests each against the block and lists the ones that reach it (their x
-// weights and their y/z weights re-indexed by block row) and one item per (atom, block row) it
-// covers; step B gives each lane one item at a time, i.e. the P contributions of one stencil row.
-// The accumulator rows have an odd stride, so the rows of one atom fall in different banks.
+// The work is split so that every lane does the same amount: a round takes up to spread_slots(P)
+// candidates; step A tests each against the block and lists the ones that reach it (their
+// weights) and one item per (atom, block row) it covers; step B gives each lane one item at a
+// time, i.e. the P contributions of one stencil row.  The accumulator rows are P-1 points longer
+// than the grid row, so a stencil row never wraps while spreading (the overhang is folded back
+// when the rows are converted), and their stride is odd, so the rows of one atom fall in
+// different banks.
 // ---------------------------------------------------------------------------------------------
-constexpr int kSpreadSlots = 2 * kThreads;          // candidates per round (listed-atom slots)
 constexpr int kSpreadMaxBlock = 4;                  // row-block edge limit (bry, brz)
-constexpr int kSpreadItemCap = kSpreadSlots * kSpreadMaxBlock * kSpreadMaxBlock;
-constexpr int kSpreadBookInts = 168;                // candidate bins, counts, offsets, counters
+constexpr int kSpreadBookInts = 168;                // counters, candidate-bin offsets and bases
+// candidates per round (listed-atom slots) and the items they can produce
+__host__ __device__ constexpr int spread_slots(int order) { return order <= 4 ? 2 * kThreads : kThreads; }
+__host__ __device__ constexpr int spread_item_cap(int order) {
+  return spread_slots(order) * kSpreadMaxBlock * kSpreadMaxBlock;
+}
 
-__host__ __device__ inline int spread_row_stride(int nx) { return nx | 1; }
+__host__ __device__ inline int spread_row_stride(int nx, int order) { return (nx + order - 1) | 1; }
 __host__ __device__ inline size_t align16(size_t b) { return (b + 15) & ~(size_t)15; }
 
 // smem of the spread + x tile: 3 x 32-bit accumulators per point, twiddles, bookkeeping, then a
 // work area that holds the listed atoms and items while spreading and the FFT buffers after.
 __host__ __device__ inline size_t spread_x_smem_bytes(int nx, int rows, int order) {
-  const size_t acc = align16((size_t)rows * spread_row_stride(nx) * 12);
+  const size_t acc = align16((size_t)rows * spread_row_stride(nx, order) * 12);
   const size_t fft = (size_t)2 * nx * (rows + 1) * sizeof(float2);
-  const size_t lists = (size_t)kSpreadSlots * (1 + order + 2 * kSpreadMaxBlock) * 4 +
-                       (size_t)kSpreadItemCap * sizeof(unsigned short);
+  const size_t lists = (size_t)spread_slots(order) * 3 * order * 4 + (size_t)spread_item_cap(order) * sizeof(unsigned int);
   return acc + align16((size_t)nx * sizeof(float2)) + kSpreadBookInts * sizeof(int) + (fft > lists ? fft : lists);
 }
 
@@ -713,10 +717,8 @@ template <int MODE>
 __device__ __forceinline__ void add_fixed(unsigned int* s0, unsigned int* s1, int* s2, int idx, long long v,
                                           int k, unsigned int kmask) {
   if (MODE == kSplit2) {
-    const unsigned int lo = (unsigned int)(unsigned long long)v & kmask;
-    const int hi = (int)(v >> k);
-    atomicAdd(&s0[idx], lo);
-    if (hi != 0) atomicAdd(&s2[idx], hi);
+    atomicAdd(&s0[idx], (unsigned int)(unsigned long long)v & kmask);
+    atomicAdd(&s2[idx], (int)(v >> k));
   } else if (MODE == kSplit3) {
     const unsigned long long u = (unsigned long long)v;
     const unsigned int p0 = (unsigned int)(u & 0xffffull), p1 = (unsigned int)((u >> 16) & 0xffffull);
@@ -733,16 +735,29 @@ __device__ __forceinline__ void add_fixed(unsigned int* s0, unsigned int* s1, in
   }
 }
 
-// The listed atoms of a round, structure of arrays over kSpreadSlots slots:
-//   ix[slot]; w[k][slot] = q thx[k] (k < P); w[P + ry][slot] = thy of block row ry;
-//   w[P + kSpreadMaxBlock + rz][slot] = thz of block row rz.
-// An item is slot | ry << 9 | rz << 11.
+// The listed atoms of a round: w[k][slot] over spread_slots(P) slots, k < 3P: q thx, thy, thz.
+// An item is slot | b << 9 | c << 12 | (row * Lp + ix) << 15: stencil indices b (y) and c (z)
+// and the accumulator offset of the stencil row's first point.
 struct SpreadLists {
-  int* ix;
   float* w;
-  unsigned short* items;
+  unsigned int* items;
   int* counters;   // [0] listed atoms, [1] items
 };
+
+// Block rows [0, nr) covered by a stencil whose first row sits at r0 in [0, n) relative to the
+// block (rows r0 .. r0+P-1, wrapped mod n), as a bitmask.
+__device__ __forceinline__ unsigned int covered_rows(int r0, int P, int n, int nr) {
+  unsigned int m = 0u;
+  if (r0 < nr) {
+    const int hi = min(nr, r0 + P);
+    m = (1u << hi) - (1u << r0);
+  }
+  if (r0 + P > n) {
+    const int hi = min(nr, r0 + P - n);
+    m |= (1u << hi) - 1u;
+  }
+  return m;
+}
 
 // First candidate bin and number of candidate bins along one axis: the origin rows
 // R0-P+1 .. R0+nr-1 (wrapped) cover the consecutive bins b0, b0+1, ..., own (mod nb), or every
@@ -766,26 +781,19 @@ __device__ __forceinline__ void cand_axis(int P, int n, int br, int nb, int own,
 template <int P>
 __device__ __forceinline__ void spread_list_atom(const SysDesc& d, bool has, const float4& head,
                                                  const float4 (&w4)[(rec_floats(P) - 8) / 4], int Y0, int Z0,
-                                                 int nry, int nrz, const SpreadLists& sl) {
-  constexpr int S = kSpreadSlots;
+                                                 int nry, int nrz, int Lp, const SpreadLists& sl) {
+  constexpr int S = spread_slots(P);
   const Geom& g = d.g;
   const int lane = threadIdx.x & 31;
-  unsigned int my = 0u, mz = 0u;   // block rows covered by the stencil
+  unsigned int my = 0u, mz = 0u;
   int ry0 = 0, rz0 = 0;
   if (has) {
     ry0 = __float_as_int(head.y) - Y0;
     if (ry0 < 0) ry0 += g.ny;
     rz0 = __float_as_int(head.z) - Z0;
     if (rz0 < 0) rz0 += g.nz;
-#pragma unroll
-    for (int b = 0; b < P; b++) {
-      int y = ry0 + b;
-      if (y >= g.ny) y -= g.ny;
-      if (y < nry) my |= 1u << y;
-      int z = rz0 + b;
-      if (z >= g.nz) z -= g.nz;
-      if (z < nrz) mz |= 1u << z;
-    }
+    my = covered_rows(ry0, P, g.ny, nry);
+    mz = covered_rows(rz0, P, g.nz, nrz);
   }
   const int nrow = __popc(my) * __popc(mz);
   const unsigned int act = __ballot_sync(0xffffffffu, nrow > 0);
@@ -805,61 +813,52 @@ __device__ __forceinline__ void spread_list_atom(const SysDesc& d, bool has, con
   sbase = __shfl_sync(0xffffffffu, sbase, 0);
   ibase = __shfl_sync(0xffffffffu, ibase, 0);
   if (nrow == 0) return;
-  const int slot = sbase + __popc(act & ((1u << lane) - 1u));
-  constexpr int NW = rec_floats(P) - 8;
-  float w[NW];
+  const unsigned int slot = sbase + __popc(act & ((1u << lane) - 1u));
+  float* ws = sl.w + slot;
 #pragma unroll
-  for (int c = 0; c < NW / 4; c++) {
-    w[4 * c] = w4[c].x;
-    w[4 * c + 1] = w4[c].y;
-    w[4 * c + 2] = w4[c].z;
-    w[4 * c + 3] = w4[c].w;
+  for (int c = 0; c < 3 * P / 4; c++) {
+    ws[(4 * c) * S] = w4[c].x;
+    ws[(4 * c + 1) * S] = w4[c].y;
+    ws[(4 * c + 2) * S] = w4[c].z;
+    ws[(4 * c + 3) * S] = w4[c].w;
   }
-  sl.ix[slot] = __float_as_int(head.x);
-#pragma unroll
-  for (int k = 0; k < P; k++) sl.w[k * S + slot] = w[k];
-#pragma unroll
-  for (int b = 0; b < P; b++) {
-    int y = ry0 + b;
-    if (y >= g.ny) y -= g.ny;
-    if (y < nry) sl.w[(P + y) * S + slot] = w[P + b];
-    int z = rz0 + b;
-    if (z >= g.nz) z -= g.nz;
-    if (z < nrz) sl.w[(P + kSpreadMaxBlock + z) * S + slot] = w[2 * P + b];
+  if ((3 * P) % 4 != 0) {   // P = 6: the last two weights
+    ws[(3 * P - 2) * S] = w4[(3 * P) / 4].x;
+    ws[(3 * P - 1) * S] = w4[(3 * P) / 4].y;
   }
-  int r = ibase + incl - nrow;
+  const unsigned int ix = (unsigned int)__float_as_int(head.x);
+  unsigned int* it = sl.items + (ibase + incl - nrow);
   unsigned int mzz = mz;
   while (mzz) {
     const int rz = __ffs(mzz) - 1;
     mzz &= mzz - 1;
+    int c = rz - rz0;
+    if (c < 0) c += g.nz;
     unsigned int myy = my;
     while (myy) {
       const int ry = __ffs(myy) - 1;
       myy &= myy - 1;
-      sl.items[r++] = (unsigned short)(slot | ry << 9 | rz << 11);
+      int b = ry - ry0;
+      if (b < 0) b += g.ny;
+      *it++ = slot | (unsigned int)b << 9 | (unsigned int)c << 12 | ((unsigned int)(ry + nry * rz) * Lp + ix) << 15;
     }
   }
 }
 
-// Step B: the P contributions of one (atom, block row) item per lane.
+// Step B: the P contributions of one (atom, stencil row) item per lane.
 template <int P, int MODE>
-__device__ __forceinline__ void spread_items(const SpreadLists& sl, int nitems, int nry, int L, int Lp,
-                                             unsigned int* s0, unsigned int* s1, int* s2, int k2,
-                                             unsigned int kmask) {
-  constexpr int S = kSpreadSlots;
+__device__ __forceinline__ void spread_items(const SpreadLists& sl, int nitems, unsigned int* s0, unsigned int* s1,
+                                             int* s2, int k2, unsigned int kmask) {
+  constexpr int S = spread_slots(P);
   for (int j = threadIdx.x; j < nitems; j += kThreads) {
     const unsigned int it = sl.items[j];
-    const int slot = it & 511u, ry = (it >> 9) & 3u, rz = it >> 11;
-    const int ix = sl.ix[slot];
-    const float ty = sl.w[(P + ry) * S + slot];
-    const float tz = sl.w[(P + kSpreadMaxBlock + rz) * S + slot];
-    const int rb = (ry + nry * rz) * Lp;
+    const float* ws = sl.w + (it & 511u);
+    const float ty = ws[(P + ((it >> 9) & 7u)) * S];
+    const float tz = ws[(2 * P + ((it >> 12) & 7u)) * S];
+    const int base = (int)(it >> 15);
 #pragma unroll
-    for (int k = 0; k < P; k++) {
-      int x = ix + k;
-      if (x >= L) x -= L;
-      add_fixed<MODE>(s0, s1, s2, rb + x, fixed_contrib(sl.w[k * S + slot], ty, tz), k2, kmask);
-    }
+    for (int k = 0; k < P; k++)
+      add_fixed<MODE>(s0, s1, s2, base + k, fixed_contrib(ws[k * S], ty, tz), k2, kmask);
   }
 }
 
@@ -867,11 +866,11 @@ template <int P>
 __device__ __forceinline__ void spread_x_tile(const SysDesc& d, int tile, int parity, char* smem_raw) {
   constexpr int RF = rec_floats(P);
   constexpr int NW4 = (RF - 8) / 4;          // float4s of spreading weights
-  constexpr int S = kSpreadSlots;
-  constexpr int PRE = P <= 4 ? 2 : 1;          // candidates whose records a thread loads at once
+  constexpr int S = spread_slots(P);
+  constexpr int PRE = S / kThreads;            // candidates whose records a thread loads at once
   const Geom& g = d.g;
   const FftPlan1D& plan = d.px;
-  const int L = g.nx, Lp = spread_row_stride(L);
+  const int L = g.nx, Lp = spread_row_stride(L, P);
   const int by = tile % d.nby, bz = tile / d.nby;
   const int Y0 = by * d.bry, Z0 = bz * d.brz;
   const int nry = min(d.bry, g.ny - Y0), nrz = min(d.brz, g.nz - Z0);
@@ -884,13 +883,13 @@ __device__ __forceinline__ void spread_x_tile(const SysDesc& d, int tile, int pa
   char* p = smem_raw + align16((size_t)rows * Lp * 12);
   float2* tw = (float2*)p;
   p += align16((size_t)L * sizeof(float2));
-  int* book = (int*)p;                         // [0..1] counters, [32..96] candidate-bin offsets
-  int* coff = book + 32;
+  int* book = (int*)p;                         // [0..1] counters, [32..96] candidate-bin offsets,
+  int* coff = book + 32;                       // [100..163] their first record (in records)
+  int* cbase = book + 100;
   p += kSpreadBookInts * sizeof(int);
   SpreadLists sl;
-  sl.ix = (int*)p;
-  sl.w = (float*)(sl.ix + S);
-  sl.items = (unsigned short*)(sl.w + (size_t)(P + 2 * kSpreadMaxBlock) * S);
+  sl.w = (float*)p;
+  sl.items = (unsigned int*)(sl.w + (size_t)3 * P * S);
   sl.counters = book;
   float2* b0 = (float2*)p;                     // FFT view of the work area (after spreading)
   float2* b1 = b0 + (size_t)L * ld;
@@ -904,7 +903,8 @@ __device__ __forceinline__ void spread_x_tile(const SysDesc& d, int tile, int pa
   cand_axis(P, g.nz, d.brz, d.nbz, bz, Z0, nrz, b0z, ncz);
   const int nc = ncy * ncz;
   if (tid < 32) {
-    // counts of the candidate bins (c = cy + ncy cz, at most 64) and their exclusive prefix
+    // counts of the candidate bins (c = cy + ncy cz, at most 64), their exclusive prefix and the
+    // index of their first record
     int n01[2], inc[2];
 #pragma unroll
     for (int h = 0; h < 2; h++) {
@@ -914,7 +914,9 @@ __device__ __forceinline__ void spread_x_tile(const SysDesc& d, int tile, int pa
         int cby = b0y + c % ncy, cbz = b0z + c / ncy;
         if (cby >= d.nby) cby -= d.nby;
         if (cbz >= d.nbz) cbz -= d.nbz;
-        n01[h] = min(__ldcg(&d.bin_count[parity * nbins + cby + d.nby * cbz]), d.bin_cap);
+        const int b = cby + d.nby * cbz;
+        n01[h] = min(__ldcg(&d.bin_count[parity * nbins + b]), d.bin_cap);
+        cbase[c] = b * d.bin_cap;
       }
       inc[h] = n01[h];
     }
@@ -961,10 +963,7 @@ __device__ __forceinline__ void spread_x_tile(const SysDesc& d, int tile, int pa
         if (q < total) {
           int c = 0;
           while (q >= coff[c + 1]) c++;
-          int cby = b0y + c % ncy, cbz = b0z + c / ncy;
-          if (cby >= d.nby) cby -= d.nby;
-          if (cbz >= d.nbz) cbz -= d.nbz;
-          rec = d.bin_recs + ((size_t)(cby + d.nby * cbz) * d.bin_cap + (q - coff[c])) * RF;
+          rec = d.bin_recs + ((size_t)cbase[c] + (q - coff[c])) * RF;
         } else if (q < ncand) {
           rec = d.ovf_recs + (size_t)(q - total) * RF;
         }
@@ -981,14 +980,14 @@ __device__ __forceinline__ void spread_x_tile(const SysDesc& d, int tile, int pa
         }
       }
 #pragma unroll
-      for (int u = 0; u < PRE; u++) spread_list_atom<P>(d, has[u], head[u], w4[u], Y0, Z0, nry, nrz, sl);
+      for (int u = 0; u < PRE; u++) spread_list_atom<P>(d, has[u], head[u], w4[u], Y0, Z0, nry, nrz, Lp, sl);
     }
     __syncthreads();
     if (base0 == 0) step_mark(d, 2);
     const int ni = sl.counters[1];
-    if (mode == kSplit2) spread_items<P, kSplit2>(sl, ni, nry, L, Lp, s0, s1, s2, k2, kmask);
-    else if (mode == kSplit3) spread_items<P, kSplit3>(sl, ni, nry, L, Lp, s0, s1, s2, k2, kmask);
-    else spread_items<P, kCarry>(sl, ni, nry, L, Lp, s0, s1, s2, k2, kmask);
+    if (mode == kSplit2) spread_items<P, kSplit2>(sl, ni, s0, s1, s2, k2, kmask);
+    else if (mode == kSplit3) spread_items<P, kSplit3>(sl, ni, s0, s1, s2, k2, kmask);
+    else spread_items<P, kCarry>(sl, ni, s0, s1, s2, k2, kmask);
     __syncthreads();
     if (tid < 2) sl.counters[tid] = 0;
     __syncthreads();
@@ -1002,12 +1001,16 @@ __device__ __forceinline__ void spread_x_tile(const SysDesc& d, int tile, int pa
   if (tid < L) tw[tid] = tw0;
   if (tid + kThreads < L) tw[tid + kThreads] = tw1;
   const int sh = mode == kSplit2 ? k2 : 32;
-  // rows: r = ry + nry*rz (r < nry*nrz valid); FFT line t = r
+  // rows: r = ry + nry*rz (r < nry*nrz valid); FFT line t = r.  Point e of a row also takes the
+  // overhang at e + L (the stencil rows that ran past the row end).
   for (int idx = tid; idx < rows * L; idx += kThreads) {
     const int t = fdiv(idx, plan.n_div), e = idx - t * L;
     const int a = t * Lp + e;
-    const unsigned long long u = (unsigned long long)s0[a] + ((unsigned long long)s1[a] << 16) +
-                                 ((unsigned long long)(long long)s2[a] << sh);
+    unsigned long long u = (unsigned long long)s0[a] + ((unsigned long long)s1[a] << 16) +
+                           ((unsigned long long)(long long)s2[a] << sh);
+    if (e < P - 1)
+      u += (unsigned long long)s0[a + L] + ((unsigned long long)s1[a + L] << 16) +
+           ((unsigned long long)(long long)s2[a + L] << sh);
     b0[e * ld + t] = make_float2(fixed_to_float((long long)u), 0.0f);
   }
   __syncthreads();
