@@ -67,7 +67,7 @@ struct pme_batch {
   unsigned long long* d_bar = nullptr;
   int* d_status = nullptr;
   size_t smem = 0;
-  int grid = 0;
+  FusedShape shape{kFusedLatency, 0};
   unsigned int spin_limit = 1u << 22;
   size_t bytes = 0;
   unsigned long long* trace = nullptr;
@@ -143,15 +143,10 @@ int launch_fused_single(pme_recip* h, const SysDesc& d_in) {
   a.nbar = fused_barriers(a.total);
   a.single = d;
   const size_t smem = fused_smem_bytes(d);
-  int grid = 0;
-  cudaError_t e = fused_max_grid(smem, &grid);
-  if (e != cudaSuccess) return cuda_fail(e, "fused: occupancy");
-  if (grid < 1) return fail(PME_EUNSUPPORTED, "fused kernel does not fit on an SM");
-  int most = 1;
-  for (int p = 0; p < kPhases; p++) most = std::max(most, a.total[p]);
-  grid = std::max(1, std::min(grid, most));
-  if (h->grid_cap > 0) grid = std::min(grid, h->grid_cap);
-  e = fused_launch(a, grid, smem, h->stream);
+  FusedShape shape;
+  cudaError_t e = fused_shape(a.total, smem, h->grid_cap, &shape);
+  if (e != cudaSuccess) return cuda_fail(e, "fused: launch shape (does the kernel fit on an SM?)");
+  e = fused_launch(a, shape, smem, h->stream);
   if (e != cudaSuccess) return cuda_fail(e, "fused eval launch");
   return PME_OK;
 }
@@ -669,14 +664,8 @@ int pme_batch_commit(pme_batch* b) {
   if (e == cudaSuccess) e = cudaMemcpy(b->d_prefix, prefix.data(), prefix.size() * sizeof(int), cudaMemcpyHostToDevice);
   if (e != cudaSuccess) return cuda_fail(e, "batch: upload descriptors");
   b->smem = smem;
-  int grid = 0;
-  e = fused_max_grid(smem, &grid);
-  if (e != cudaSuccess) return cuda_fail(e, "batch: occupancy");
-  if (grid < 1) return fail(PME_EUNSUPPORTED, "batch: kernel does not fit on an SM");
-  int most = 1;
-  for (int p = 0; p < kPhases; p++) most = std::max(most, b->total[p]);
-  b->grid = std::min(grid, most);
-  if (b->grid_cap > 0) b->grid = std::min(b->grid, b->grid_cap);
+  e = fused_shape(b->total, smem, b->grid_cap, &b->shape);
+  if (e != cudaSuccess) return cuda_fail(e, "batch: launch shape (does the kernel fit on an SM?)");
   return PME_OK;
 }
 
@@ -709,7 +698,7 @@ int pme_batch_eval(pme_batch* b) {
   a.spin_limit = b->spin_limit;
   a.trace = b->trace;
   a.trace_ctas = b->trace_ctas;
-  cudaError_t e = fused_launch(a, b->grid, b->smem, b->stream);
+  cudaError_t e = fused_launch(a, b->shape, b->smem, b->stream);
   if (e != cudaSuccess) return cuda_fail(e, "batch eval launch");
   return PME_OK;
 }
@@ -742,7 +731,7 @@ int pme_batch_get_energy_virial(pme_batch* b, double* out) {
 int pme_batch_info(const pme_batch* b, int* nsys, int* grid, size_t* device_bytes) {
   if (!b) return fail(PME_EINVAL, "batch is NULL");
   if (nsys) *nsys = (int)b->desc.size();
-  if (grid) *grid = b->grid;
+  if (grid) *grid = b->shape.grid;
   if (device_bytes) *device_bytes = b->bytes;
   return PME_OK;
 }

@@ -5,9 +5,9 @@
 // accesses are conflict free).  The transform is a Stockham autosort FFT: stage s with radix R
 // reads butterfly j's inputs at j + r*L/R, twiddles them by W_{Ns R}^{r k} (k = j mod Ns), does an
 // R-point DFT in registers and writes the outputs at (j div Ns) Ns R + k + u Ns, ping-ponging
-// between two buffers.  Radices 2, 3, 4, 5 cover every 2/3/5-smooth length.  Twiddles
-// W_L^i = exp(-2 pi i i/L) are read from a per-length table computed in FP64 on the host and
-// rounded to FP32.  sign = -1 forward, +1 inverse; transforms are unnormalised.
+// between two buffers.  Radices 8, 4, 2, 3, 5 (largest power of two first) cover every
+// 2/3/5-smooth length.  Twiddles W_L^i = exp(-2 pi i i/L) are read from a per-length table
+// computed in FP64 on the host and rounded to FP32.  sign = -1 forward, +1 inverse; transforms are unnormalised.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -110,6 +110,31 @@ template <> __device__ __forceinline__ void dft_small<5>(float2* v, bool inv) {
   v[3] = csub(r2, j2);
 }
 
+// 8-point DFT as two 4-point DFTs of the even and odd inputs, joined by the twiddles W_8^k:
+// forward W_8 = (1 - i)/sqrt(2), W_8^2 = -i, W_8^3 = -(1 + i)/sqrt(2); inverse the conjugates.
+template <> __device__ __forceinline__ void dft_small<8>(float2* v, bool inv) {
+  const float r = 0.707106781186547524400844f;   // 1/sqrt(2)
+  float2 e[4] = {v[0], v[2], v[4], v[6]};
+  float2 o[4] = {v[1], v[3], v[5], v[7]};
+  dft_small<4>(e, inv);
+  dft_small<4>(o, inv);
+  // o[1] *= W_8, o[2] *= W_8^2, o[3] *= W_8^3
+  const float2 a = o[1], c = o[3];
+  if (!inv) {
+    o[1] = make_float2(__fmul_rn(__fadd_rn(a.x, a.y), r), __fmul_rn(__fsub_rn(a.y, a.x), r));
+    o[3] = make_float2(__fmul_rn(__fsub_rn(c.y, c.x), r), -__fmul_rn(__fadd_rn(c.x, c.y), r));
+  } else {
+    o[1] = make_float2(__fmul_rn(__fsub_rn(a.x, a.y), r), __fmul_rn(__fadd_rn(a.x, a.y), r));
+    o[3] = make_float2(-__fmul_rn(__fadd_rn(c.x, c.y), r), __fmul_rn(__fsub_rn(c.x, c.y), r));
+  }
+  o[2] = cmul_si(o[2], inv);
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    v[k] = cadd(e[k], o[k]);
+    v[k + 4] = csub(e[k], o[k]);
+  }
+}
+
 // Thread placement inside a tile: line t = tid mod nlines, butterfly lane y = tid div nlines
 // (lanes 0..ny-1; threads beyond nlines*ny idle during stages).
 struct TileLane {
@@ -164,6 +189,7 @@ __device__ __forceinline__ float2* fft_tile(float2* buf0, float2* buf1, const Ff
     const int R = plan.radix[s];
     const FastDiv nsd = plan.ns_div[s];
     switch (R) {
+      case 8: fft_stage<8>(src, dst, L, Ns, nsd, es, ls, ln, tw, inv); break;
       case 4: fft_stage<4>(src, dst, L, Ns, nsd, es, ls, ln, tw, inv); break;
       case 2: fft_stage<2>(src, dst, L, Ns, nsd, es, ls, ln, tw, inv); break;
       case 3: fft_stage<3>(src, dst, L, Ns, nsd, es, ls, ln, tw, inv); break;

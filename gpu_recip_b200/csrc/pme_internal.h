@@ -51,7 +51,15 @@ cudaError_t staged_solve(const SysDesc& d, cudaStream_t s);
 cudaError_t staged_c2r(const SysDesc& d, cudaStream_t s);
 cudaError_t staged_gather(const SysDesc& d, cudaStream_t s);
 
-cudaError_t fused_launch(const FusedArgs& a, int grid, size_t smem, cudaStream_t s);
-cudaError_t fused_max_grid(size_t smem, int* grid);
+// Launch shape of a fused evaluation: which build of the kernel and how many CTAs.
+enum { kFusedLatency = 0, kFusedThroughput = 1 };
+struct FusedShape {
+  int variant;
+  int grid;
+};
+// Picks the build and the CTAs (at most the resident maximum, at most the largest phase's tile
+// count, at most grid_cap when > 0) for phases of total[] tiles and smem bytes per CTA.
+cudaError_t fused_shape(const int* total, size_t smem, int grid_cap, FusedShape* out);
+cudaError_t fused_launch(const FusedArgs& a, const FusedShape& shape, size_t smem, cudaStream_t s);
 
 }  // namespace pme

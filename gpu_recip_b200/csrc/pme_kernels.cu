@@ -171,7 +171,8 @@ __device__ __forceinline__ int find_system(const int* prefix, int nsys, int t) {
   return lo;
 }
 
-__global__ void __launch_bounds__(kThreads) k_fused(FusedArgs a) {
+// The fused evaluation's body; compiled twice (see k_fused_lat / k_fused_tput below).
+__device__ __forceinline__ void fused_body(const FusedArgs& a) {
   __shared__ SysDesc d;
   __shared__ int cur;
   extern __shared__ float2 smem[];
@@ -230,6 +231,13 @@ __global__ void __launch_bounds__(kThreads) k_fused(FusedArgs a) {
     }
   }
 }
+
+// Latency build: up to 128 registers, 2 CTAs of 256 threads per SM; for launches with about one
+// tile per CTA in a phase.  Throughput build: at most 80 registers, 3 CTAs per SM (a few spills in
+// the largest tiles); for launches with many tiles per CTA, where the extra resident warps hide
+// more latency than the spills cost.
+__global__ void __launch_bounds__(kThreads) k_fused_lat(FusedArgs a) { fused_body(a); }
+__global__ void __launch_bounds__(kThreads, 3) k_fused_tput(FusedArgs a) { fused_body(a); }
 
 // ------------------------------- host launchers ----------------------------------------------
 static size_t staged_fft_smem(int L, int tx) { return tile_smem_bytes(L, tx) + 32 * 7 * sizeof(long long); }
@@ -325,22 +333,36 @@ cudaError_t staged_gather(const SysDesc& d, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-cudaError_t fused_launch(const FusedArgs& a, int grid, size_t smem, cudaStream_t s) {
-  FusedArgs args = a;
-  args.gather_wide = a.total[kPhases - 1] <= grid ? 1 : 0;
-  void* params[] = {&args};
-  return cudaLaunchCooperativeKernel((const void*)k_fused, dim3(grid), dim3(kThreads), params, smem, s);
+static const void* fused_kernel(int variant) {
+  return variant == kFusedThroughput ? (const void*)k_fused_tput : (const void*)k_fused_lat;
 }
 
-cudaError_t fused_max_grid(size_t smem, int* grid) {
-  int dev = 0, sms = 0, per_sm = 0;
+cudaError_t fused_shape(const int* total, size_t smem, int grid_cap, FusedShape* out) {
+  int dev = 0, sms = 0, occ_lat = 0, occ_tput = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
-  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fused, kThreads, smem)) != cudaSuccess)
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_lat, k_fused_lat, kThreads, smem)) != cudaSuccess)
     return e;
-  *grid = sms * per_sm;
-  return cudaSuccess;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_tput, k_fused_tput, kThreads, smem)) != cudaSuccess)
+    return e;
+  int most = 1;
+  for (int p = 0; p < kPhases; p++) most = most > total[p] ? most : total[p];
+  // many tiles per CTA: more resident CTAs pay; about one: fewer registers per thread cost
+  const bool tput = occ_tput > occ_lat && most > 2 * sms * occ_lat;
+  out->variant = tput ? kFusedThroughput : kFusedLatency;
+  int grid = sms * (tput ? occ_tput : occ_lat);
+  grid = grid < most ? grid : most;
+  if (grid_cap > 0 && grid > grid_cap) grid = grid_cap;
+  out->grid = grid;
+  return grid >= 1 ? cudaSuccess : cudaErrorInvalidConfiguration;
+}
+
+cudaError_t fused_launch(const FusedArgs& a, const FusedShape& shape, size_t smem, cudaStream_t s) {
+  FusedArgs args = a;
+  args.gather_wide = a.total[kPhases - 1] <= shape.grid ? 1 : 0;
+  void* params[] = {&args};
+  return cudaLaunchCooperativeKernel(fused_kernel(shape.variant), dim3(shape.grid), dim3(kThreads), params, smem, s);
 }
 
 // Opt every dynamic-shared-memory kernel in to the device's per-CTA budget (minus the kernel's
@@ -365,9 +387,10 @@ cudaError_t configure_kernels(size_t* max_dyn_smem) {
   if ((e = opt_in_smem(k_x_inv, optin)) != cudaSuccess) return e;
   if ((e = opt_in_smem(k_ypass, optin)) != cudaSuccess) return e;
   if ((e = opt_in_smem(k_zpass, optin)) != cudaSuccess) return e;
-  if ((e = opt_in_smem(k_fused, optin)) != cudaSuccess) return e;
+  if ((e = opt_in_smem(k_fused_lat, optin)) != cudaSuccess) return e;
+  if ((e = opt_in_smem(k_fused_tput, optin)) != cudaSuccess) return e;
   cudaFuncAttributes fa;
-  if ((e = cudaFuncGetAttributes(&fa, k_fused)) != cudaSuccess) return e;
+  if ((e = cudaFuncGetAttributes(&fa, k_fused_lat)) != cudaSuccess) return e;
   if (max_dyn_smem) *max_dyn_smem = (size_t)optin - fa.sharedSizeBytes;
   return cudaSuccess;
 }

@@ -225,7 +225,7 @@ struct pme_server {
   int* h_status = nullptr;                 // pinned: device status after each step, by parity
   int total[kPhases] = {0};
   size_t smem = 0;
-  int grid = 0;
+  FusedShape shape{kFusedLatency, 0};
   cudaEvent_t step_ev[2] = {nullptr, nullptr};
   int step_parity = 0;
   // requests
@@ -328,12 +328,8 @@ int rebuild(pme_server* s) {
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(s->d_slots, st + align256(tb) + align256(pb), sb, cudaMemcpyHostToDevice, s->stream);
   if (e != cudaSuccess) return cuda_fail(e, "server: upload tables");
-  int grid = 0;
-  e = fused_max_grid(s->smem, &grid);
-  if (e != cudaSuccess) return cuda_fail(e, "server: occupancy");
-  int most = 1;
-  for (int p = 0; p < kPhases; p++) most = std::max(most, s->total[p]);
-  s->grid = std::max(1, std::min(grid, most));
+  e = fused_shape(s->total, s->smem, 0, &s->shape);
+  if (e != cudaSuccess) return cuda_fail(e, "server: launch shape");
   return PME_OK;
 }
 
@@ -356,7 +352,7 @@ int step(pme_server* s) {
   a.bar = s->d_bar;
   a.status = s->d_status;
   a.spin_limit = s->spin_limit;
-  e = fused_launch(a, s->grid, s->smem, s->stream);
+  e = fused_launch(a, s->shape, s->smem, s->stream);
   if (e != cudaSuccess) return cuda_fail(e, "server: fused launch");
   k_server_post<<<n, 32, 0, s->stream>>>(s->d_slots, n);
   e = cudaGetLastError();

@@ -49,6 +49,7 @@ inline bool factorize(int n, FftPlan1D& p) {
     m /= r;
     return true;
   };
+  while (m % 8 == 0) if (!push(8)) return false;
   while (m % 4 == 0) if (!push(4)) return false;
   while (m % 2 == 0) if (!push(2)) return false;
   while (m % 3 == 0) if (!push(3)) return false;
