@@ -478,6 +478,9 @@ __device__ __forceinline__ void z_tile(const SysDesc& d, int mode, int tile, flo
   const size_t es = (size_t)g.ny;
   if (mode != 3)
     for (int i = tid; i < L; i += kThreads) tw[i] = __ldg(&d.tw[plan.tw_off + i]);
+  // the solve's influence tables load together with the columns (their own smem region)
+  KTab kt;
+  if (mode == 2 || mode == 3) kt = stage_ktab(d, kx, ksm);
   for (int idx = tid; idx < L * tx; idx += kThreads) {
     const int e = fdiv(idx, txd), t = idx - e * tx;
     b0[e * ld + t] = t < nt ? __ldcg(&base[e * es + t]) : make_float2(0.0f, 0.0f);
@@ -488,8 +491,6 @@ __device__ __forceinline__ void z_tile(const SysDesc& d, int mode, int tile, flo
   if (mode == 0 || mode == 2) res = fft_tile(b0, b1, plan, ld, 1, ln, tw, false);
   if (mode == 1) res = fft_tile(b0, b1, plan, ld, 1, ln, tw, true);
   if (mode == 2 || mode == 3) {
-    const KTab kt = stage_ktab(d, kx, ksm);
-    __syncthreads();
     long long acc[7] = {0, 0, 0, 0, 0, 0, 0};
     for (int idx = tid; idx < L * tx; idx += kThreads) {
       const int e = fdiv(idx, txd), t = idx - e * tx;
