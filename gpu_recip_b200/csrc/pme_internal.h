@@ -31,7 +31,6 @@ struct FusedArgs {
   int nbar;                  // grid barriers per launch (non-empty phases - 1)
   unsigned long long* trace; // optional: [cta][phase][begin, end] %globaltimer stamps
   int trace_ctas;            // CTAs recorded (rows of trace)
-  int gather_wide;           // set by fused_launch: 1 when the gather phase has <= 1 tile per CTA
 };
 
 cudaError_t configure_kernels(size_t* max_dyn_smem);

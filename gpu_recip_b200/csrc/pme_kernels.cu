@@ -219,7 +219,7 @@ __device__ __forceinline__ void fused_body(const FusedArgs& a) {
           if (local < tiles_xpass(d)) x_inv_tile(d, local, smem);
           else if (threadIdx.x == 0) finalize_system(d, true, true);
           break;
-        default: gather_bin_dispatch(d, local, parity, (char*)smem, a.gather_wide != 0); break;
+        default: gather_bin_dispatch(d, local, parity, (char*)smem); break;
       }
       __syncthreads();
     }
@@ -360,7 +360,6 @@ cudaError_t fused_shape(const int* total, size_t smem, int grid_cap, FusedShape*
 
 cudaError_t fused_launch(const FusedArgs& a, const FusedShape& shape, size_t smem, cudaStream_t s) {
   FusedArgs args = a;
-  args.gather_wide = a.total[kPhases - 1] <= shape.grid ? 1 : 0;
   void* params[] = {&args};
   return cudaLaunchCooperativeKernel(fused_kernel(shape.variant), dim3(shape.grid), dim3(kThreads), params, smem, s);
 }

@@ -91,8 +91,8 @@ __host__ __device__ inline int tiles_zpass(const SysDesc& d) { return ((d.g.ny +
 __host__ __device__ inline int tiles_plane(const SysDesc& d) { return d.g.hx; }
 __host__ __device__ inline int tiles_bin(const SysDesc& d) { return (d.natom + kThreads - 1) / kThreads; }
 __host__ __device__ inline int tiles_blocks(const SysDesc& d) { return d.nby * d.nbz; }
-// Lanes per atom of the latency-oriented gather (staged gather, fused launches with about one
-// gather tile per CTA): as few as keep the rows of one lane, P^2 / lanes, at 8-9.
+// Lanes per atom of the gather (staged and fused): as few as keep the rows of one lane,
+// P^2 / lanes, at 8-9, so that a bin's atoms take few passes.
 __host__ __device__ constexpr int gather_lanes(int order) { return order <= 4 ? 2 : (order <= 6 ? 4 : 8); }
 constexpr int kGatherAtoms = kThreads / 8;   // staged gather tile: atoms of the smallest pass
 __host__ __device__ inline int tiles_gather(const SysDesc& d) {
@@ -1290,29 +1290,19 @@ __device__ __forceinline__ void gather_dispatch(const SysDesc& d, int tile) {
 }
 
 template <int P>
-__device__ __forceinline__ void gather_bin_any(const SysDesc& d, int tile, int parity, int* red, bool wide) {
-  if (wide) {
-    switch (d.force_kind) {
-      case kForceF32Soa: gather_bin_tile<P, kForceF32Soa, gather_lanes(P)>(d, tile, parity, red); break;
-      case kForceF32x3: gather_bin_tile<P, kForceF32x3, gather_lanes(P)>(d, tile, parity, red); break;
-      default: gather_bin_tile<P, kForceI64SoaAccum, gather_lanes(P)>(d, tile, parity, red); break;
-    }
-  } else {
-    switch (d.force_kind) {
-      case kForceF32Soa: gather_bin_tile<P, kForceF32Soa, 8>(d, tile, parity, red); break;
-      case kForceF32x3: gather_bin_tile<P, kForceF32x3, 8>(d, tile, parity, red); break;
-      default: gather_bin_tile<P, kForceI64SoaAccum, 8>(d, tile, parity, red); break;
-    }
+__device__ __forceinline__ void gather_bin_any(const SysDesc& d, int tile, int parity, int* red) {
+  switch (d.force_kind) {
+    case kForceF32Soa: gather_bin_tile<P, kForceF32Soa, gather_lanes(P)>(d, tile, parity, red); break;
+    case kForceF32x3: gather_bin_tile<P, kForceF32x3, gather_lanes(P)>(d, tile, parity, red); break;
+    default: gather_bin_tile<P, kForceI64SoaAccum, gather_lanes(P)>(d, tile, parity, red); break;
   }
 }
 
-// wide: gather_lanes(P) lanes per atom (few passes per bin: for launches with about one gather
-// tile per CTA); otherwise 8 (fewer partly-filled warps: for launches with many tiles per CTA).
-__device__ __forceinline__ void gather_bin_dispatch(const SysDesc& d, int tile, int parity, char* smem, bool wide) {
+__device__ __forceinline__ void gather_bin_dispatch(const SysDesc& d, int tile, int parity, char* smem) {
   switch (d.order) {
-    case 4: gather_bin_any<4>(d, tile, parity, (int*)smem, wide); break;
-    case 6: gather_bin_any<6>(d, tile, parity, (int*)smem, wide); break;
-    default: gather_bin_any<8>(d, tile, parity, (int*)smem, wide); break;
+    case 4: gather_bin_any<4>(d, tile, parity, (int*)smem); break;
+    case 6: gather_bin_any<6>(d, tile, parity, (int*)smem); break;
+    default: gather_bin_any<8>(d, tile, parity, (int*)smem); break;
   }
 }
 
