@@ -899,13 +899,13 @@ __device__ __forceinline__ void spread_x_tile(const SysDesc& d, int tile, int pa
   // twiddles: loaded now, stored to smem once the spreading is done (L <= 2 kThreads)
   const float2 tw0 = tid < L ? __ldg(&d.tw[plan.tw_off + tid]) : make_float2(0.0f, 0.0f);
   const float2 tw1 = tid + kThreads < L ? __ldg(&d.tw[plan.tw_off + tid + kThreads]) : make_float2(0.0f, 0.0f);
-  int b0y, ncy, b0z, ncz;
-  cand_axis(P, g.ny, d.bry, d.nby, by, Y0, nry, b0y, ncy);
-  cand_axis(P, g.nz, d.brz, d.nbz, bz, Z0, nrz, b0z, ncz);
-  const int nc = ncy * ncz;
   if (tid < 32) {
     // counts of the candidate bins (c = cy + ncy cz, at most 64), their exclusive prefix and the
     // index of their first record
+    int b0y, ncy, b0z, ncz;
+    cand_axis(P, g.ny, d.bry, d.nby, by, Y0, nry, b0y, ncy);
+    cand_axis(P, g.nz, d.brz, d.nbz, bz, Z0, nrz, b0z, ncz);
+    const int nc = ncy * ncz;
     int n01[2], inc[2];
 #pragma unroll
     for (int h = 0; h < 2; h++) {
@@ -935,15 +935,17 @@ __device__ __forceinline__ void spread_x_tile(const SysDesc& d, int tile, int pa
     if (tid == 31) coff[64] = tot0 + inc[1];
     if (tid < 2) sl.counters[tid] = 0;
   }
-  for (int idx = tid; idx < rows * Lp; idx += kThreads) {
-    s0[idx] = 0u;
-    s1[idx] = 0u;
-    s2[idx] = 0;
+  {
+    // the three accumulator arrays are one 16-byte-aligned block of 3 rows*Lp words
+    const int words = 3 * rows * Lp;
+    uint4* z4 = (uint4*)s0;
+    for (int i = tid; i < words / 4; i += kThreads) z4[i] = make_uint4(0u, 0u, 0u, 0u);
+    for (int i = (words & ~3) + tid; i < words; i += kThreads) s0[i] = 0u;
   }
   const int novf = __ldcg(&d.bin_meta[kMetaOvf + parity]);
   const float qmax = __int_as_float(__ldcg(&d.bin_meta[kMetaQmax + parity]));
   __syncthreads();
-  const int total = coff[nc];
+  const int total = coff[64];
   step_mark(d, 1);
   const int ncand = total + novf;
   // accumulation form for this tile (see add_fixed)
