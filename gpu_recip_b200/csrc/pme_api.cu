@@ -443,7 +443,7 @@ int pme_copy_charge_grid(pme_recip* h, float* host_out) {
   std::vector<long long> tmp(h->st.G());
   int rc = copy_back(h, tmp.data(), h->st.accum, h->st.G() * 8, "copy_charge_grid");
   if (rc) return rc;
-  for (size_t i = 0; i < tmp.size(); i++) host_out[i] = (float)((double)tmp[i] * kInvFixedScale);
+  for (size_t i = 0; i < tmp.size(); i++) host_out[i] = (float)tmp[i] * kInvFixedScaleF;   // as fixed_to_float
   return PME_OK;
 }
 

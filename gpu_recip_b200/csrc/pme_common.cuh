@@ -15,6 +15,7 @@ constexpr double kCcelec = 332.0716;          // 1/(4 pi eps0) in kcal/mol A/e^2
 constexpr double kPi = 3.14159265358979323846;
 constexpr float kFixedScale = 1099511627776.0f;        // 2^40: grid fixed point
 constexpr double kInvFixedScale = 1.0 / 1099511627776.0;
+constexpr float kInvFixedScaleF = 1.0f / 1099511627776.0f;   // 2^-40, exact
 constexpr int kMaxOrder = 8;
 
 // Per-system geometry in the form the kernels use.
@@ -84,8 +85,11 @@ __device__ __forceinline__ long long fixed_contrib(float qthx, float thy, float 
   return __float2ll_rn(__fmul_rn(v, kFixedScale));
 }
 
+// Fixed point -> FP32 in FP32 arithmetic: v rounded once to the nearest float, then scaled by
+// 2^-40, which is exact (|v| >= 1 stays far from the subnormal range).  Equal to rounding the exact
+// quotient v * 2^-40 once.
 __device__ __forceinline__ float fixed_to_float(long long v) {
-  return (float)((double)v * kInvFixedScale);
+  return __fmul_rn(__ll2float_rn(v), kInvFixedScaleF);
 }
 
 __device__ __forceinline__ int wrap_add(int i, int a, int n) {

@@ -951,8 +951,9 @@ __device__ __forceinline__ void spread_x_tile(const SysDesc& d, int tile, int pa
   // accumulation form for this tile (see add_fixed)
   const int k2 = __clz(max(ncand, 1));          // largest k with ncand 2^k < 2^32
   const unsigned int kmask = (unsigned int)((1ull << k2) - 1ull);
-  const double hib = (double)ncand * ((double)qmax * ldexp(1.0, 40 - k2) * 1.001 + 2.0);
-  const int mode = hib < 2147483648.0 ? kSplit2 : (ncand <= 65536 ? kSplit3 : kCarry);
+  // hi-sum bound in FP32 (the 1.001 covers its rounding); NaN or inf qmax fails the test
+  const float hib = (float)ncand * __fmaf_rn(qmax, ldexpf(1.001f, 40 - k2), 2.0f);
+  const int mode = hib < 2147483648.0f ? kSplit2 : (ncand <= 65536 ? kSplit3 : kCarry);
   for (int base0 = 0; base0 < ncand; base0 += S) {
 #pragma unroll 1
     for (int h0 = 0; h0 < S; h0 += PRE * kThreads) {

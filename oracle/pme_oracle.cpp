@@ -233,9 +233,10 @@ extern "C" int orc_spread_fixed(const float* xyzq, int natom, const double* reci
   return 0;
 }
 
-// int64 fixed point -> FP32 grid value (one rounding of the exact quotient).
+// int64 fixed point -> FP32 grid value: the integer rounded once to float (round to nearest),
+// then scaled by 2^-40 (exact), i.e. one rounding of the exact quotient.
 extern "C" int orc_fixed_to_float(const int64_t* in, size_t n, float* out) {
-  for (size_t i = 0; i < n; i++) out[i] = (float)((double)in[i] * 0x1p-40);
+  for (size_t i = 0; i < n; i++) out[i] = (float)in[i] * 0x1p-40f;
   return 0;
 }
 
