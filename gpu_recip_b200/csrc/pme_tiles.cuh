@@ -106,35 +106,6 @@ __host__ inline size_t tile_smem_bytes(int L, int tx) {
 // ---------------------------------------------------------------------------------------------
 // Block reductions
 // ---------------------------------------------------------------------------------------------
-template <int K>
-__device__ __forceinline__ void warp_sum(double (&v)[K]) {
-#pragma unroll
-  for (int off = 16; off >= 1; off >>= 1)
-#pragma unroll
-    for (int c = 0; c < K; c++) v[c] += __shfl_down_sync(0xffffffffu, v[c], off);
-}
-
-// Deterministic block sum; the result is valid in thread 0.  `scratch` holds 32*K doubles.
-template <int K>
-__device__ __forceinline__ void block_sum(double (&v)[K], double* scratch) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  warp_sum<K>(v);
-  __syncthreads();
-  if (lane == 0)
-#pragma unroll
-    for (int c = 0; c < K; c++) scratch[warp * K + c] = v[c];
-  __syncthreads();
-  if (warp == 0) {
-#pragma unroll
-    for (int c = 0; c < K; c++) v[c] = lane < nw ? scratch[lane * K + c] : 0.0;
-    warp_sum<K>(v);
-  }
-}
-
-__device__ __forceinline__ void acc_add(long long* acc, int slot, double v, double scale) {
-  atomicAdd((unsigned long long*)&acc[slot], (unsigned long long)__double2ll_rn(v * scale));
-}
-
 // Block sum of one int64 per thread; the result is valid in thread 0.  `scratch`: 32 int64.
 __device__ __forceinline__ long long block_sum_ll(long long v, long long* scratch) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
