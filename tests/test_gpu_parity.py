@@ -284,3 +284,28 @@ def test_atom_count_change_on_one_handle(cuda):
         want = _run(cuda, sys_)
         assert np.array_equal(got["force"], want["force"]), sys_.name
         assert got["energy"] == want["energy"] and np.array_equal(got["virial"], want["virial"])
+
+
+def _clustered():
+    """3,000 atoms, 2,400 of them packed into a 4 A cube: their row blocks overflow the fixed bin
+    capacity, so spread and gather go through the overflow list."""
+    rng = np.random.default_rng(44)
+    box = (30.0, 30.0, 30.0)
+    x = np.empty((3000, 4), np.float32)
+    x[:2400, :3] = 10.0 + 4.0 * rng.random((2400, 3))
+    x[2400:, :3] = 30.0 * rng.random((600, 3))
+    x[:, 3] = np.where(np.arange(3000) % 3 == 0, -0.834, 0.417)
+    return S.PmeSystem("clustered", x, box, (32, 32, 32), 4, 0.34)
+
+
+def test_bin_overflow_path(cuda, oracle):
+    s = _clustered()
+    a = _run(cuda, s, staged=True)
+    b = _run(cuda, s)
+    c = _run(cuda, s, pme=b["pme"])          # second evaluation walks the bin-sorted order
+    ref = oracle.evaluate(s.xyzq.astype(np.float64), s.recip3, s.nfft, s.order, s.kappa)
+    assert _rel_rms(b["force"], ref["force"]) <= FORCE_RMS_TOL
+    assert abs(b["energy"] - ref["energy"]) <= ENERGY_REL_TOL * abs(ref["energy"])
+    for got in (b, c):
+        assert np.array_equal(a["force"], got["force"])
+        assert a["energy"] == got["energy"] and np.array_equal(a["virial"], got["virial"])
