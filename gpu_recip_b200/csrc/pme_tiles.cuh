@@ -748,72 +748,84 @@ __device__ __forceinline__ void cand_axis(int P, int n, int br, int nb, int own,
   cnt += 1;
 }
 
-// Step A for one candidate per lane, its record already loaded (has == false: no candidate).
-// Every lane of the warp calls it.
-template <int P>
-__device__ __forceinline__ void spread_list_atom(const SysDesc& d, bool has, const float4& head,
-                                                 const float4 (&w4)[(rec_floats(P) - 8) / 4], int Y0, int Z0,
-                                                 int nry, int nrz, int Lp, const SpreadLists& sl) {
+// Step A for PRE candidates per lane, their records already loaded (has[u] == false: none).
+// The lane's listed atoms and items are reserved together: one warp scan and one pair of counter
+// updates per warp.  Every lane of the warp calls it.
+template <int P, int PRE>
+__device__ __forceinline__ void spread_list_atoms(const SysDesc& d, const bool (&has)[PRE], const float4 (&head)[PRE],
+                                                  const float4 (&w4)[PRE][(rec_floats(P) - 8) / 4], int Y0, int Z0,
+                                                  int nry, int nrz, int Lp, const SpreadLists& sl) {
   constexpr int S = spread_slots(P);
   const Geom& g = d.g;
   const int lane = threadIdx.x & 31;
-  unsigned int my = 0u, mz = 0u;
-  int ry0 = 0, rz0 = 0;
-  if (has) {
-    ry0 = __float_as_int(head.y) - Y0;
-    if (ry0 < 0) ry0 += g.ny;
-    rz0 = __float_as_int(head.z) - Z0;
-    if (rz0 < 0) rz0 += g.nz;
-    my = covered_rows(ry0, P, g.ny, nry);
-    mz = covered_rows(rz0, P, g.nz, nrz);
+  unsigned int my[PRE], mz[PRE];
+  int ry0[PRE], rz0[PRE], nrow[PRE];
+  int v = 0;   // this lane's items (low 16 bits) and listed atoms (high bits)
+#pragma unroll
+  for (int u = 0; u < PRE; u++) {
+    my[u] = mz[u] = 0u;
+    ry0[u] = rz0[u] = 0;
+    if (has[u]) {
+      ry0[u] = __float_as_int(head[u].y) - Y0;
+      if (ry0[u] < 0) ry0[u] += g.ny;
+      rz0[u] = __float_as_int(head[u].z) - Z0;
+      if (rz0[u] < 0) rz0[u] += g.nz;
+      my[u] = covered_rows(ry0[u], P, g.ny, nry);
+      mz[u] = covered_rows(rz0[u], P, g.nz, nrz);
+    }
+    nrow[u] = __popc(my[u]) * __popc(mz[u]);
+    v += nrow[u] + (nrow[u] > 0 ? 1 << 16 : 0);
   }
-  const int nrow = __popc(my) * __popc(mz);
-  const unsigned int act = __ballot_sync(0xffffffffu, nrow > 0);
-  if (act == 0u) return;
-  int incl = nrow;
+  int incl = v;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
     const int t = __shfl_up_sync(0xffffffffu, incl, o);
     if (lane >= o) incl += t;
   }
   const int wtot = __shfl_sync(0xffffffffu, incl, 31);
+  if (wtot == 0) return;
   int sbase = 0, ibase = 0;
   if (lane == 0) {
-    sbase = atomicAdd(&sl.counters[0], __popc(act));
-    ibase = atomicAdd(&sl.counters[1], wtot);
+    sbase = atomicAdd(&sl.counters[0], wtot >> 16);
+    ibase = atomicAdd(&sl.counters[1], wtot & 0xffff);
   }
   sbase = __shfl_sync(0xffffffffu, sbase, 0);
   ibase = __shfl_sync(0xffffffffu, ibase, 0);
-  if (nrow == 0) return;
-  const unsigned int slot = sbase + __popc(act & ((1u << lane) - 1u));
-  float* ws = sl.w + slot;
+  const int excl = incl - v;
+  unsigned int slot = (unsigned int)(sbase + (excl >> 16));
+  unsigned int* it = sl.items + (ibase + (excl & 0xffff));
 #pragma unroll
-  for (int c = 0; c < 3 * P / 4; c++) {
-    ws[(4 * c) * S] = w4[c].x;
-    ws[(4 * c + 1) * S] = w4[c].y;
-    ws[(4 * c + 2) * S] = w4[c].z;
-    ws[(4 * c + 3) * S] = w4[c].w;
-  }
-  if ((3 * P) % 4 != 0) {   // P = 6: the last two weights
-    ws[(3 * P - 2) * S] = w4[(3 * P) / 4].x;
-    ws[(3 * P - 1) * S] = w4[(3 * P) / 4].y;
-  }
-  const unsigned int ix = (unsigned int)__float_as_int(head.x);
-  unsigned int* it = sl.items + (ibase + incl - nrow);
-  unsigned int mzz = mz;
-  while (mzz) {
-    const int rz = __ffs(mzz) - 1;
-    mzz &= mzz - 1;
-    int c = rz - rz0;
-    if (c < 0) c += g.nz;
-    unsigned int myy = my;
-    while (myy) {
-      const int ry = __ffs(myy) - 1;
-      myy &= myy - 1;
-      int b = ry - ry0;
-      if (b < 0) b += g.ny;
-      *it++ = slot | (unsigned int)b << 9 | (unsigned int)c << 12 | ((unsigned int)(ry + nry * rz) * Lp + ix) << 15;
+  for (int u = 0; u < PRE; u++) {
+    if (nrow[u] == 0) continue;
+    float* ws = sl.w + slot;
+#pragma unroll
+    for (int c = 0; c < 3 * P / 4; c++) {
+      ws[(4 * c) * S] = w4[u][c].x;
+      ws[(4 * c + 1) * S] = w4[u][c].y;
+      ws[(4 * c + 2) * S] = w4[u][c].z;
+      ws[(4 * c + 3) * S] = w4[u][c].w;
     }
+    if ((3 * P) % 4 != 0) {   // P = 6: the last two weights
+      ws[(3 * P - 2) * S] = w4[u][(3 * P) / 4].x;
+      ws[(3 * P - 1) * S] = w4[u][(3 * P) / 4].y;
+    }
+    const unsigned int ix = (unsigned int)__float_as_int(head[u].x);
+    unsigned int mzz = mz[u];
+    while (mzz) {
+      const int rz = __ffs(mzz) - 1;
+      mzz &= mzz - 1;
+      int c = rz - rz0[u];
+      if (c < 0) c += g.nz;
+      unsigned int myy = my[u];
+      while (myy) {
+        const int ry = __ffs(myy) - 1;
+        myy &= myy - 1;
+        int b = ry - ry0[u];
+        if (b < 0) b += g.ny;
+        *it++ = slot | (unsigned int)b << 9 | (unsigned int)c << 12 | ((unsigned int)(ry + nry * rz) * Lp + ix) << 15;
+      }
+    }
+    slot++;
   }
 }
 
@@ -954,8 +966,7 @@ __device__ __forceinline__ void spread_x_tile(const SysDesc& d, int tile, int pa
           for (int c = 0; c < NW4; c++) w4[u][c] = head[u];
         }
       }
-#pragma unroll
-      for (int u = 0; u < PRE; u++) spread_list_atom<P>(d, has[u], head[u], w4[u], Y0, Z0, nry, nrz, Lp, sl);
+      spread_list_atoms<P, PRE>(d, has, head, w4, Y0, Z0, nry, nrz, Lp, sl);
     }
     __syncthreads();
     if (base0 == 0) step_mark(d, 2);
