@@ -4,14 +4,16 @@
 //  * staged kernels, one tile per CTA, one launch per reference stage (spread_charge, r2c_fft,
 //    scalar_sum, c2r_fft, gather_force, calc_self_energy of CudaPMERecip.cu);
 //  * the persistent fused kernel: one cooperative launch runs every phase of every system of a
-//    batch, with bounded grid barriers between phases:
-//      0 spread (+ sum q^2) and the FP64 influence tables      (:479-580, :1252-1275)
-//      1 x pass forward, int64 -> FP32, accumulation grid re-zeroed  (cuFFT R2C :2421)
-//      2 y pass forward
-//      3 z pass forward + solve with energy/virial + z inverse  (:594-901)
-//      4 y pass inverse, and the energy/virial finalisation
-//      5 x pass inverse (C2R)                                   (cuFFT C2R :2464)
-//      6 gather                                                  (:1031-1245)
+//    batch, with bounded grid barriers between non-empty phases:
+//      0 bin atoms by row block (records, sum q^2, max |q|) and the FP64 influence tables
+//                                                                    (:479-580, :1252-1275)
+//      1 spread into one row block in shared memory, x forward       (cuFFT R2C :2421)
+//      2 y forward, or whole kx planes: y, z, solve, z and y inverse (:594-901)
+//      3 z forward + solve with energy/virial + z inverse (no planes)
+//      4 y inverse (no planes)
+//      5 x inverse (C2R) and the energy/virial finalisation          (cuFFT C2R :2464)
+//      6 gather by bin, writing the bin-sorted atom order            (:1031-1245)
+//    It is compiled twice (latency and throughput builds, see k_fused_lat / k_fused_tput).
 // Both forms execute the same per-element arithmetic, so forces and energies agree bit for bit.
 #include <cuda_runtime.h>
 #include <stdint.h>

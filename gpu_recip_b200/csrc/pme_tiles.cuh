@@ -3,10 +3,10 @@
 // barriers between phases).  Every function assumes blockDim.x == kThreads and must be called
 // by all threads of the CTA (they synchronise internally).
 //
-// Energy, virial and sum(q^2) are reduced in FP64 inside the CTA, then added to per-system int64
-// fixed-point accumulators (scale 2^32 for energy/virial, 2^40 for sum(q^2)).  Integer addition is
-// associative, so the totals are bit-identical for any tiling, launch shape or batch mix; a
-// finalize step converts them into the FP64 energy/virial record.
+// Energy and virial terms are rounded per element to integers at scale 2^32 and sum(q^2) per atom
+// at 2^40; they are summed as int64 inside the CTA and added to per-system int64 accumulators.
+// Integer addition is associative, so the totals are bit-identical for any tiling, launch shape
+// or batch mix; a finalize step converts them into the FP64 energy/virial record.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -74,6 +74,9 @@ struct SysDesc {
 };
 
 // Profiling stamp of one step of a tile (CTA 0, thread 0 only; no-op when steps is null).
+// Slots: 0-6 the spread + x tile (start, candidates counted, first round listed, spreading done,
+// rows converted, x FFT done, stored), 8-14 the plane tile, 16-21 the bin tile, 24-26 the gather
+// tile; a CTA that runs several tiles of a phase leaves the stamps of its last one.
 __device__ __forceinline__ void step_mark(const SysDesc& d, int slot) {
   if (d.steps != nullptr && blockIdx.x == 0 && threadIdx.x == 0) {
     unsigned long long t;
