@@ -128,6 +128,14 @@ __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long
   return v;
 }
 
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+
 __device__ __forceinline__ void red_release_add_u64(unsigned long long* p, unsigned long long v) {
   asm volatile("red.release.gpu.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
@@ -146,14 +154,18 @@ __device__ bool grid_barrier(unsigned long long* bar, unsigned long long base, i
     red_release_add_u64(&bar[0], 1ull);
     int good = 1;
     unsigned int it = 0;
-    while (ld_acquire_u64(&bar[0]) < target) {
-      if (++it > spin_limit || ld_volatile(status) != 0) {
+    // relaxed polls, then one acquire fence once the count is reached (the acquire pattern); the
+    // status word (another CTA gave up) is looked at every 64 polls
+    while (ld_relaxed_u64(&bar[0]) < target) {
+      ++it;
+      if (it > spin_limit || ((it & 63u) == 0u && ld_volatile(status) != 0)) {
         atomicCAS(status, 0, kStatusBarrierTimeout);
         good = 0;
         break;
       }
       if (it > 64) __nanosleep(32);
     }
+    fence_acq_rel_gpu();
     if (good && k == 0 && blockIdx.x == 0) {
       bar[1] = base + (unsigned long long)nbar * gridDim.x;
       bar[3] = bar[3] + 1ull;   // launch counter (bin parity); every CTA read it before barrier 0
