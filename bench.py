@@ -394,7 +394,7 @@ def run_batched(args, dev, stream, flush, rank, world):
             "p50_ms": float(np.percentile(per, 50)), "p99_ms": float(np.percentile(per, 99)),
             "launches_per_batch": 1, "cuda_graph": True, "grid_ctas": info["grid_ctas"],
             "autotune": {"schedule": ["auto", "planes", "passes"][tune["schedule"]], "grid_ctas": tune["grid_ctas"],
-                         "candidates": tune["candidates"]},
+                         "line_scale": tune["x_lines"], "candidates": tune["candidates"]},
             "device_bytes": info["device_bytes"], "alg_bytes_per_batch": alg,
             "roofline_frac": alg / (ms * 1e-3) / 1e9 / peak}
 

@@ -74,6 +74,7 @@ struct pme_batch {
   int trace_ctas = 0;
   int plane_mode = 0;   // PME_SCHED_*: AUTO and PLANES use planes where they fit
   int grid_cap = 0;
+  int line_scale = 1;   // lines per x/y/z pass tile: each system's default times this (budget permitting)
 };
 
 namespace {
@@ -187,6 +188,14 @@ void set_config(pme_recip* h, const pme_tune_config& c) {
   h->st.tx_y = c.y_lines;
   h->st.tx_z = c.z_columns;
   h->grid_cap = c.grid_ctas;
+}
+
+// base * scale lines per pass tile, at most limit, shrunk (not below base) until the tile's
+// shared memory (plus `extra` bytes) fits the budget.
+int scaled_lines(int L, int base, int scale, int limit, size_t extra) {
+  int t = std::min(base * scale, std::max(limit, base));
+  while (t > base && tile_smem_bytes(L, t) + extra > kTileSmemBudget) t--;
+  return t;
 }
 
 void apply_cached_config(pme_recip* h) {
@@ -651,7 +660,12 @@ int pme_batch_commit(pme_batch* b) {
   std::vector<int> prefix((size_t)kPhases * (nsys + 1), 0);
   size_t smem = 0;
   for (int i = 0; i < nsys; i++) {
-    b->desc[i].plane = (b->st[i].plane && b->plane_mode != PME_SCHED_PASSES) ? 1 : 0;
+    const SystemState& st = b->st[i];
+    b->desc[i].plane = (st.plane && b->plane_mode != PME_SCHED_PASSES) ? 1 : 0;
+    b->desc[i].tx_rows = scaled_lines(st.nx, st.tx_rows, b->line_scale, 64, 0);
+    b->desc[i].tx_y = scaled_lines(st.ny, st.tx_y, b->line_scale, 64, 0);
+    b->desc[i].tx_z = scaled_lines(st.nz, st.tx_z, b->line_scale, std::max(st.tx_z, st.ny),
+                                   ktab_smem_bytes(st.ny, st.nz));
     int cnt[kPhases];
     fused_tile_counts(b->desc[i], cnt);
     for (int p = 0; p < kPhases; p++)
@@ -934,28 +948,34 @@ int pme_batch_autotune(pme_batch* b, int reps, pme_tune_config* out) {
   if (e == cudaSuccess) e = ev.init();
   if (e != cudaSuccess) return cuda_fail(e, "batch autotune: setup");
   const int sms = sm_count(b->device);
-  const int start_mode = b->plane_mode, start_cap = b->grid_cap;
-  int best_mode = start_mode, best_cap = start_cap, count = 0, rc = PME_OK;
+  const int start_mode = b->plane_mode, start_cap = b->grid_cap, start_scale = b->line_scale;
+  int best_mode = start_mode, best_cap = start_cap, best_scale = start_scale, count = 0, rc = PME_OK;
   float best_us = 0.0f;
-  for (int mode : {PME_SCHED_AUTO, PME_SCHED_PASSES}) {
-    for (int cap : {0, sms}) {
-      b->plane_mode = mode;
-      b->grid_cap = cap;
-      if ((rc = pme_batch_commit(b))) break;
-      float us = 0.0f;
-      rc = time_launches([&]() { return pme_batch_eval(b); }, b->stream, b->d_status, reps, ev, &us);
-      if (rc) break;
-      if (count == 0 || us < 0.98f * best_us) {
-        best_us = us;
-        best_mode = mode;
-        best_cap = cap;
+  for (int scale : {1, 2, 4}) {
+    for (int mode : {PME_SCHED_AUTO, PME_SCHED_PASSES}) {
+      for (int cap : {0, sms}) {
+        b->plane_mode = mode;
+        b->grid_cap = cap;
+        b->line_scale = scale;
+        if ((rc = pme_batch_commit(b))) break;
+        float us = 0.0f;
+        rc = time_launches([&]() { return pme_batch_eval(b); }, b->stream, b->d_status, reps, ev, &us);
+        if (rc) break;
+        if (count == 0 || us < 0.98f * best_us) {
+          best_us = us;
+          best_mode = mode;
+          best_cap = cap;
+          best_scale = scale;
+        }
+        count++;
       }
-      count++;
+      if (rc) break;
     }
     if (rc) break;
   }
   b->plane_mode = rc == PME_OK ? best_mode : start_mode;
   b->grid_cap = rc == PME_OK ? best_cap : start_cap;
+  b->line_scale = rc == PME_OK ? best_scale : start_scale;
   const int rc2 = pme_batch_commit(b);
   e = cudaStreamSynchronize(b->stream);
   for (size_t i = 0; i < nsys && e == cudaSuccess; i++)
@@ -967,6 +987,7 @@ int pme_batch_autotune(pme_batch* b, int reps, pme_tune_config* out) {
     std::memset(out, 0, sizeof(*out));
     out->schedule = best_mode;
     out->grid_ctas = best_cap;
+    out->x_lines = out->y_lines = out->z_columns = best_scale;   // multiplier of each system's default
     out->us_per_eval = best_us;
     out->candidates = count;
   }

@@ -201,10 +201,12 @@ PME_API int pme_batch_get_energy_virial(pme_batch* b, double* out);
 PME_API int pme_batch_info(const pme_batch* b, int* nsys, int* grid_ctas, size_t* device_bytes);
 PME_API int pme_batch_set_trace(pme_batch* b, unsigned long long* dev_buf, int max_ctas);
 /* Autotune the batch's launch: the y/z schedule of every system (planes where they fit, or
- * passes) and the CTAs of the launch, `reps` timed evaluations per candidate; the fastest is kept
- * (and committed).  The evaluations write the systems' force outputs as pme_batch_eval does (int64
- * outputs accumulate every tuning evaluation: clear them afterwards); the energy/virial records are
- * left as they were.  out may be NULL; out->x_lines, y_lines and z_columns are 0 (per system). */
+ * passes), the lines per x/y/z pass tile (each system's default times 1, 2 or 4, within the
+ * shared-memory budget) and the CTAs of the launch, `reps` timed evaluations per candidate; the
+ * fastest is kept (and committed).  The evaluations write the systems' force outputs as
+ * pme_batch_eval does (int64 outputs accumulate every tuning evaluation: clear them afterwards);
+ * the energy/virial records are left as they were.  out may be NULL; out->x_lines, y_lines and
+ * z_columns hold the chosen multiplier. */
 PME_API int pme_batch_autotune(pme_batch* b, int reps, pme_tune_config* out);
 /* Device bytes one system of this grid occupies (for admission by HBM footprint). */
 PME_API size_t pme_system_device_bytes(int nfftx, int nffty, int nfftz);
