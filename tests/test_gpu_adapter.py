@@ -1,0 +1,79 @@
+"""The MD-side callers of the path: CudaDomdecRecip::calc with its three force outputs
+(CudaDomdecRecip.h:50-81), the int64 output accumulating onto forces already there (as direct-space
+forces would be), and the recip node's request loop (CudaDomdecRecipLooper::run) in process."""
+import threading
+
+import numpy as np
+import pytest
+
+from gpu_recip_b200 import systems as S
+
+pytestmark = pytest.mark.gpu
+
+
+def _fixed(f):
+    return np.rint(f.astype(np.float64) * 2.0 ** 40).astype(np.int64)
+
+
+def test_domdec_recip_three_force_kinds_and_int64_accumulate(cuda):
+    torch = cuda
+    from gpu_recip_b200 import CudaDomdecRecip, force_stride
+    s = S.config_small(seed=5)
+    n = s.natom
+    rec = CudaDomdecRecip(*s.nfft, s.order, s.kappa)
+    x = torch.from_numpy(s.xyzq).cuda()
+    inv = [1.0 / b for b in s.box]
+    f3 = torch.zeros((n, 3), dtype=torch.float32, device="cuda")
+    rec.calc(*inv, x, n, True, True, f3)
+    st = force_stride(n)
+    fs = torch.zeros(3 * st, dtype=torch.float32, device="cuda")
+    rec.calc(*inv, x, n, True, True, fs, st)
+    st8 = force_stride(n, 8)
+    prior = np.random.default_rng(3).integers(-2 ** 45, 2 ** 45, size=(3, st8)).astype(np.int64)
+    fi = torch.from_numpy(prior.copy().reshape(-1)).cuda()
+    rec.calc(*inv, x, n, True, True, fi, st8)
+    torch.cuda.synchronize()
+    a = f3.cpu().numpy()
+    b = fs.view(3, st)[:, :n].T.cpu().numpy()
+    assert np.array_equal(a, b)
+    got = fi.view(3, st8).cpu().numpy()
+    want = prior.copy()
+    want[:, :n] += _fixed(a).T
+    assert np.array_equal(got, want)
+
+
+def test_recip_looper_serves_a_direct_node(cuda):
+    torch = cuda
+    from gpu_recip_b200 import CudaDomdecRecip
+    from gpu_recip_b200.looper import InProcessRecipComm, RecipLooper
+    s = S.config_small(seed=9)
+    comm = InProcessRecipComm(timeout=120.0)
+    looper = RecipLooper(comm, *s.nfft, s.order, s.kappa)
+    out = {}
+    th = threading.Thread(target=lambda: out.setdefault("steps", looper.run()))
+    th.start()
+    rng = np.random.default_rng(11)
+    ref = CudaDomdecRecip(*s.nfft, s.order, s.kappa)
+    try:
+        for step, (scale, e, v) in enumerate([(1.0, True, True), (1.01, False, True), (0.995, True, False)]):
+            box = [b * scale for b in s.box]
+            x = s.xyzq.copy()
+            x[:, :3] += rng.normal(0.0, 0.05, size=(s.natom, 3)).astype(np.float32)
+            n = s.natom - 7 * step                      # the coordinate count may change per step
+            xd = torch.from_numpy(x[:n].copy()).cuda()
+            comm.send_header(n, *[1.0 / b for b in box], e, v)
+            comm.send_coord(xd)
+            reply = comm.recv_force()
+            want = torch.zeros((n, 3), dtype=torch.float32, device="cuda")
+            ev = ref.pme.energy_virial
+            ev.clear()
+            ref.calc(*[1.0 / b for b in box], xd, n, e, v, want)
+            torch.cuda.synchronize()
+            ev.copyToHost()
+            assert np.array_equal(reply.force.cpu().numpy(), want.cpu().numpy())
+            assert reply.energy_virial[0] == ev.getEnergy("recip")
+            assert np.array_equal(reply.energy_virial[2:].reshape(3, 3), ev.getVirial())
+    finally:
+        comm.send_stop()
+        th.join(timeout=120)
+    assert not th.is_alive() and out["steps"] == 3
