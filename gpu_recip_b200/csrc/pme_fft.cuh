@@ -178,9 +178,9 @@ __device__ __forceinline__ void fft_stage(const float2* __restrict__ in, float2*
 // Full transform of every line of the tile held in buf0 (element stride es, line stride ls);
 // returns the buffer that holds the result (buf0 or buf1).  Every thread of the CTA must call
 // it; it synchronises between stages and before returning.
-__device__ __forceinline__ float2* fft_tile(float2* buf0, float2* buf1, const FftPlan1D& plan,
-                                            int es, int ls, const TileLane& ln, const float2* tw,
-                                            bool inv) {
+static __device__ __noinline__ float2* fft_tile(float2* buf0, float2* buf1, const FftPlan1D& plan,
+                                         int es, int ls, const TileLane ln, const float2* tw,
+                                         bool inv) {
   float2* src = buf0;
   float2* dst = buf1;
   int Ns = 1;
