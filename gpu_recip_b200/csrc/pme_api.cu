@@ -113,13 +113,6 @@ int ensure_bins(pme_recip* h, int natom) {
   return PME_OK;
 }
 
-// 3 doubles of the reciprocal diagonal
-void diag3(const double* recip, double* r3) {
-  r3[0] = recip[0];
-  r3[1] = recip[4];
-  r3[2] = recip[8];
-}
-
 int launch_fused_single(pme_recip* h, const SysDesc& d_in) {
   SysDesc d = d_in;
   FusedArgs a;
@@ -308,11 +301,9 @@ int pme_spread_charge(pme_recip* h, const void* xyzq, int ncoord, const double* 
   if (ncoord < 0 || (ncoord > 0 && !xyzq)) return fail(PME_EINVAL, "bad xyzq/ncoord");
   if (int rc = check_recip(recip)) return rc;
   DeviceGuard dg(h->device);
-  double r3[3];
-  diag3(recip, r3);
   cudaError_t e = cudaMemsetAsync(h->st.accum, 0, h->st.G() * 8, h->stream);
   if (e != cudaSuccess) return cuda_fail(e, "spread_charge: clear grid");
-  e = staged_spread(h->st.desc(r3, 0.0, xyzq, ncoord, nullptr, 0, 0, 0, 0), h->stream);
+  e = staged_spread(h->st.desc9(recip, 0.0, xyzq, ncoord, nullptr, 0, 0, 0, 0), h->stream);
   if (e != cudaSuccess) return cuda_fail(e, "spread_charge");
   h->accum_dirty = true;
   return PME_OK;
@@ -332,10 +323,8 @@ int pme_scalar_sum(pme_recip* h, const double* recip, double kappa, int calc_ene
   if (int rc = check_recip(recip)) return rc;
   if (!(kappa > 0.0) || !std::isfinite(kappa)) return fail(PME_EINVAL, "kappa must be positive");
   DeviceGuard dg(h->device);
-  double r3[3];
-  diag3(recip, r3);
   const int ev = (calc_energy || calc_virial) ? 1 : 0;
-  cudaError_t e = staged_solve(h->st.desc(r3, kappa, nullptr, 0, nullptr, 0, 0, ev, 0), h->stream);
+  cudaError_t e = staged_solve(h->st.desc9(recip, kappa, nullptr, 0, nullptr, 0, 0, ev, 0), h->stream);
   if (e != cudaSuccess) return cuda_fail(e, "scalar_sum");
   return PME_OK;
 }
@@ -355,9 +344,7 @@ int pme_gather_force(pme_recip* h, const void* xyzq, int ncoord, const double* r
   if (int rc = check_recip(recip)) return rc;
   if (int rc = check_force_args(ncoord, stride, kind, force)) return rc;
   DeviceGuard dg(h->device);
-  double r3[3];
-  diag3(recip, r3);
-  cudaError_t e = staged_gather(h->st.desc(r3, 0.0, xyzq, ncoord, force, kind, stride, 0, 0), h->stream);
+  cudaError_t e = staged_gather(h->st.desc9(recip, 0.0, xyzq, ncoord, force, kind, stride, 0, 0), h->stream);
   if (e != cudaSuccess) return cuda_fail(e, "gather_force");
   return PME_OK;
 }
@@ -414,9 +401,14 @@ int pme_energy_virial_device_ptr(pme_recip* h, double** dev_ptr) {
 int pme_eval_ortho(pme_recip* h, double inv_boxx, double inv_boxy, double inv_boxz, const void* xyzq,
                    int ncoord, double kappa, int calc_energy, int calc_virial, int kind, void* force,
                    int stride) {
+  const double recip[9] = {inv_boxx, 0, 0, 0, inv_boxy, 0, 0, 0, inv_boxz};
+  return pme_eval(h, recip, xyzq, ncoord, kappa, calc_energy, calc_virial, kind, force, stride);
+}
+
+int pme_eval(pme_recip* h, const double* recip, const void* xyzq, int ncoord, double kappa,
+             int calc_energy, int calc_virial, int kind, void* force, int stride) {
   if (int rc = handle_ok(h)) return rc;
   if (ncoord < 0 || (ncoord > 0 && !xyzq)) return fail(PME_EINVAL, "bad xyzq/ncoord");
-  const double recip[9] = {inv_boxx, 0, 0, 0, inv_boxy, 0, 0, 0, inv_boxz};
   if (int rc = check_recip(recip)) return rc;
   if (!(kappa > 0.0) || !std::isfinite(kappa)) return fail(PME_EINVAL, "kappa must be positive");
   if (int rc = check_force_args(ncoord, stride, kind, force)) return rc;
@@ -427,9 +419,8 @@ int pme_eval_ortho(pme_recip* h, double inv_boxx, double inv_boxy, double inv_bo
     h->accum_dirty = false;
   }
   if (int rc = ensure_bins(h, ncoord)) return rc;
-  const double r3[3] = {inv_boxx, inv_boxy, inv_boxz};
   const int ev = (calc_energy || calc_virial) ? 1 : 0;
-  SysDesc d = h->st.desc(r3, kappa, xyzq, ncoord, force, kind, stride, ev, calc_energy ? 1 : 0);
+  SysDesc d = h->st.desc9(recip, kappa, xyzq, ncoord, force, kind, stride, ev, calc_energy ? 1 : 0);
   return launch_fused_single(h, d);
 }
 

@@ -25,17 +25,14 @@ struct Geom {
   float rx, ry, rz;     // reciprocal box diagonal, FP32
   float sx_hi, sy_hi, sz_hi;   // n_d * r_d as a float-float pair (hi + lo), used to map a
   float sx_lo, sy_lo, sz_lo;   // coordinate to grid units without losing its low bits
+  int tric;                    // 1: triclinic box (a reciprocal matrix with off-diagonals)
+  float shi[9], slo[9];        // triclinic: S[j][d] = n_d R[j][d] (index 3 j + d) as hi + lo
 };
 
-// Fractional coordinate of one axis in grid units: fr = n * frac(x*r + 1/2) in [0, n), split into
-// the stencil origin i0 and the offset u in [0, 1].  This is the function of
-// CudaPMERecip.cu:510-529 (fr = n (w - (floor(w + 0.5) - 0.5)), w = x r + 2), evaluated without
-// its FP32 cancellation: t = x (s_hi + s_lo) + n/2 is formed as p + e with p = fl(x s_hi) and
-// e = x s_lo + (x s_hi - p) exactly recovered with an FMA, so u carries ~1e-7 grid units of
-// error instead of ~1e-5.  Non-finite or huge inputs map to i0 = 0, u = 0.
-__device__ __forceinline__ void frac_coord(float x, float s_hi, float s_lo, int n, int& i0, float& u) {
-  float p = __fmul_rn(x, s_hi);
-  float e = __fmaf_rn(x, s_lo, __fmaf_rn(x, s_hi, -p));
+// Grid-unit coordinate t = p + e (p the leading float, e its small correction, both already
+// carrying the n/2 shift of w = x r + 2 modulo n) -> stencil origin i0 and offset u in [0, 1].
+// Non-finite or huge inputs map to i0 = 0, u = 0.
+__device__ __forceinline__ void frac_finish(float p, float e, int n, int& i0, float& u) {
   if (!(fabsf(p) < 16777216.0f)) { p = 0.0f; e = 0.0f; }
   const float fl = floorf(p);
   float f = __fsub_rn(p, fl);
@@ -48,6 +45,52 @@ __device__ __forceinline__ void frac_coord(float x, float s_hi, float s_lo, int 
   if (i < 0) i += n;
   i0 = i;
   u = v;
+}
+
+// Fractional coordinate of one axis in grid units: fr = n * frac(x*r + 1/2) in [0, n), split into
+// the stencil origin i0 and the offset u in [0, 1].  This is the function of
+// CudaPMERecip.cu:510-529 (fr = n (w - (floor(w + 0.5) - 0.5)), w = x r + 2), evaluated without
+// its FP32 cancellation: t = x (s_hi + s_lo) + n/2 is formed as p + e with p = fl(x s_hi) and
+// e = x s_lo + (x s_hi - p) exactly recovered with an FMA, so u carries ~1e-7 grid units of
+// error instead of ~1e-5.
+__device__ __forceinline__ void frac_coord(float x, float s_hi, float s_lo, int n, int& i0, float& u) {
+  const float p = __fmul_rn(x, s_hi);
+  const float e = __fmaf_rn(x, s_lo, __fmaf_rn(x, s_hi, -p));
+  frac_finish(p, e, n, i0, u);
+}
+
+// Triclinic axis d: t = x S[0][d] + y S[1][d] + z S[2][d] in float-float.  Each product is split
+// into its rounded value and exact error as in frac_coord, the three leading parts are summed with
+// two error-free two-sums (Knuth), and all error terms go into e.  With S[1][d] = S[2][d] = 0 this
+// is frac_coord bit for bit.
+__device__ __forceinline__ void frac_coord_tric(float x, float y, float z, const float* shi,
+                                                const float* slo, int d, int n, int& i0, float& u) {
+  const float p0 = __fmul_rn(x, shi[d]), p1 = __fmul_rn(y, shi[3 + d]), p2 = __fmul_rn(z, shi[6 + d]);
+  const float e0 = __fmaf_rn(x, slo[d], __fmaf_rn(x, shi[d], -p0));
+  const float e1 = __fmaf_rn(y, slo[3 + d], __fmaf_rn(y, shi[3 + d], -p1));
+  const float e2 = __fmaf_rn(z, slo[6 + d], __fmaf_rn(z, shi[6 + d], -p2));
+  const float s01 = __fadd_rn(p0, p1);
+  const float b01 = __fsub_rn(s01, p0);
+  const float t01 = __fadd_rn(__fsub_rn(p0, __fsub_rn(s01, b01)), __fsub_rn(p1, b01));
+  const float p = __fadd_rn(s01, p2);
+  const float b2 = __fsub_rn(p, s01);
+  const float t2 = __fadd_rn(__fsub_rn(s01, __fsub_rn(p, b2)), __fsub_rn(p2, b2));
+  const float e = __fadd_rn(__fadd_rn(__fadd_rn(e0, e1), e2), __fadd_rn(t01, t2));
+  frac_finish(p, e, n, i0, u);
+}
+
+// Stencil origins and offsets of one atom on all three axes (orthorhombic or triclinic box).
+__device__ __forceinline__ void frac_coords(const Geom& g, float x, float y, float z, int& ix, int& iy,
+                                            int& iz, float& ux, float& uy, float& uz) {
+  if (!g.tric) {
+    frac_coord(x, g.sx_hi, g.sx_lo, g.nx, ix, ux);
+    frac_coord(y, g.sy_hi, g.sy_lo, g.ny, iy, uy);
+    frac_coord(z, g.sz_hi, g.sz_lo, g.nz, iz, uz);
+  } else {
+    frac_coord_tric(x, y, z, g.shi, g.slo, 0, g.nx, ix, ux);
+    frac_coord_tric(x, y, z, g.shi, g.slo, 1, g.ny, iy, uy);
+    frac_coord_tric(x, y, z, g.shi, g.slo, 2, g.nz, iz, uz);
+  }
 }
 
 // Cardinal B-spline weights of order P at offset u (weights of grid points i0..i0+P-1), built

@@ -130,14 +130,31 @@ inline int check_grid(int nx, int ny, int nz, int order) {
   return PME_OK;
 }
 
+inline bool recip_is_ortho(const double* recip) {
+  return recip[1] == 0.0 && recip[2] == 0.0 && recip[3] == 0.0 && recip[5] == 0.0 && recip[6] == 0.0 &&
+         recip[7] == 0.0;
+}
+
+inline double det3(const double* m) {
+  return m[0] * (m[4] * m[8] - m[5] * m[7]) - m[1] * (m[3] * m[8] - m[5] * m[6]) +
+         m[2] * (m[3] * m[7] - m[4] * m[6]);
+}
+
+// Orthorhombic recip (CudaPMERecip.cu:2042-2045 accepts only these): a finite, positive diagonal.
+// Triclinic recip R[j][d] = recip[3 j + d] (the inverse of the matrix whose rows are the box
+// vectors): finite entries and a finite, non-zero determinant.
 inline int check_recip(const double* recip) {
   if (!recip) return fail(PME_EINVAL, "recip is NULL");
-  if (!(recip[1] == 0.0 && recip[2] == 0.0 && recip[3] == 0.0 && recip[5] == 0.0 &&
-        recip[6] == 0.0 && recip[7] == 0.0))
-    return fail(PME_EINVAL, "only orthorhombic boxes are supported (recip off-diagonals must be 0)");
-  for (int i : {0, 4, 8})
-    if (!(recip[i] > 0.0) || !std::isfinite(recip[i]))
-      return fail(PME_EINVAL, "recip diagonal must be finite and positive");
+  for (int i = 0; i < 9; i++)
+    if (!std::isfinite(recip[i])) return fail(PME_EINVAL, "recip entries must be finite");
+  if (recip_is_ortho(recip)) {
+    for (int i : {0, 4, 8})
+      if (!(recip[i] > 0.0)) return fail(PME_EINVAL, "recip diagonal must be positive");
+    return PME_OK;
+  }
+  const double det = det3(recip);
+  if (!(det != 0.0) || !std::isfinite(det))
+    return fail(PME_EINVAL, "recip matrix is singular (box vectors must span a volume)");
   return PME_OK;
 }
 
@@ -176,7 +193,7 @@ struct SystemState {
   static size_t bytes(int nx, int ny, int nz) {
     const size_t G = (size_t)nx * ny * nz, H = (size_t)(nx / 2 + 1) * ny * nz, n = nx + ny + nz;
     return align256(G * 8) + align256(H * 8) + align256(G * 4) + align256(n * 8) + align256(n * 8) +
-           align256(2 * n * 8) + align256(kAccCount * 8) + align256(kEvCount * 8);
+           align256(4 * n * 8) + align256(kAccCount * 8) + align256(kEvCount * 8);
   }
 
   void setup(int nx_, int ny_, int nz_, int order_) {
@@ -224,7 +241,7 @@ struct SystemState {
     rgrid = (float*)p; p += align256(G() * 4);
     tw = (float2*)p; p += align256(n * 8);
     bmod = (double*)p; p += align256(n * 8);
-    ktab = (double*)p; p += align256(2 * n * 8);
+    ktab = (double*)p; p += align256(4 * n * 8);
     acc = (long long*)p; p += align256(kAccCount * 8);
     ev = (double*)p;
   }
@@ -307,6 +324,42 @@ struct SystemState {
       d.ovf_recs = (float*)(d.bin_meta + kMetaInts);
       d.perm = (int*)(d.ovf_recs + (size_t)std::max(atom_cap, 1) * rec_floats(kMaxOrder));
     }
+    return d;
+  }
+
+  // Descriptor from a full reciprocal matrix R[j][d] = recip9[3 j + d] (or null for setup-only
+  // calls).  A diagonal matrix gives exactly desc(diagonal); off-diagonals switch the tiles to
+  // their triclinic forms: float-float S = n_d R[j][d] for the fractional coordinates and the force
+  // transform, R and the metric G = R^T R for the influence tables, V = 1 / |det R|.
+  SysDesc desc9(const double* recip9, double kappa, const void* xyzq, int natom, void* force, int kind,
+                int stride, int calc_ev, int calc_self) const {
+    if (!recip9) return desc(nullptr, kappa, xyzq, natom, force, kind, stride, calc_ev, calc_self);
+    const double r3[3] = {recip9[0], recip9[4], recip9[8]};
+    SysDesc d = desc(r3, kappa, xyzq, natom, force, kind, stride, calc_ev, calc_self);
+    if (recip_is_ortho(recip9)) return d;
+    Geom& g = d.g;
+    g.tric = 1;
+    const int n3[3] = {nx, ny, nz};
+    for (int j = 0; j < 3; j++)
+      for (int c = 0; c < 3; c++) {
+        const double sv = recip9[3 * j + c] * n3[c];
+        g.shi[3 * j + c] = (float)sv;
+        g.slo[3 * j + c] = (float)(sv - (double)g.shi[3 * j + c]);
+      }
+    double G[9];
+    for (int a = 0; a < 3; a++)
+      for (int b = 0; b < 3; b++) {
+        double sum = 0.0;
+        for (int j = 0; j < 3; j++) sum += recip9[3 * j + a] * recip9[3 * j + b];
+        G[3 * a + b] = sum;
+      }
+    for (int i = 0; i < 9; i++) d.rm[i] = recip9[i];
+    for (int a = 0; a < 3; a++) d.gdiag[a] = G[4 * a];
+    d.cross_f[0] = (float)(-2.0 * d.fac * G[1]);
+    d.cross_f[1] = (float)(-2.0 * d.fac * G[2]);
+    d.cross_f[2] = (float)(-2.0 * d.fac * G[5]);
+    d.piv_inv = std::fabs(det3(recip9)) / kPi;
+    d.piv_inv_f = (float)d.piv_inv;
     return d;
   }
 };

@@ -42,6 +42,9 @@ struct SysDesc {
   double piv_inv;            // 1 / (pi V)
   float fac_f, piv_inv_f;    // the same, FP32
   double rxd, ryd, rzd;      // reciprocal box diagonal, FP64
+  double rm[9];              // triclinic: reciprocal matrix R[j][d] (index 3 j + d), FP64
+  double gdiag[3];           // triclinic: metric diagonal G_dd = sum_j R[j][d]^2
+  float cross_f[3];          // triclinic: -2 fac G_xy, -2 fac G_xz, -2 fac G_yz
   int calc_ev;               // energy + virial in the solve
   int calc_self;             // self energy in the spread phase
   double self_coef;          // -kappa ccelec / sqrt(pi)
@@ -155,9 +158,7 @@ __device__ __forceinline__ void spread_tile(const SysDesc& d, int tile, void* sm
     const float4 a = __ldg(&d.xyzq[base + lane]);
     SplineAtom<P>& s = sh[warp * APW + lane];
     float ux, uy, uz, th[P];
-    frac_coord(a.x, g.sx_hi, g.sx_lo, g.nx, s.ix, ux);
-    frac_coord(a.y, g.sy_hi, g.sy_lo, g.ny, s.iy, uy);
-    frac_coord(a.z, g.sz_hi, g.sz_lo, g.nz, s.iz, uz);
+    frac_coords(g, a.x, a.y, a.z, s.ix, s.iy, s.iz, ux, uy, uz);
     bspline<P>(ux, th, nullptr);
 #pragma unroll
     for (int i = 0; i < P; i++) s.tx[i] = __fmul_rn(a.w, th[i]);
@@ -283,21 +284,34 @@ __device__ __forceinline__ void x_inv_tile(const SysDesc& d, int tile, float2* s
 // eterm = exp(-fac |mhat|^2) piv_inv b_x b_y b_z / |mhat|^2.  exp(-fac |mhat|^2) b_x b_y b_z factors
 // per axis, so ktab_tile precomputes mhat_d[k] and A_d[k] = b_d[k] exp(-fac mhat_d[k]^2) in FP64
 // once per evaluation (nx+ny+nz values) and the solve evaluates eterm in FP64 from them.
+// Triclinic boxes: k = R m = sum_d m_d R[.][d], so each axis contributes a vector; |k|^2 =
+// sum_dd' G_dd' m_d m_d' (G = R^T R) keeps the per-axis factors A_d = b_d exp(-fac G_dd m_d^2) and
+// adds one cross factor exp(-2 fac (G_xy m_x m_y + G_xz m_x m_z + G_yz m_y m_z)) per element.
+// Table layout (ntot = nx+ny+nz entries each): [0] k_x contribution (mhat_d when orthorhombic),
+// [1] A_d, and for triclinic boxes [2] k_y and [3] k_z contributions.
 // ---------------------------------------------------------------------------------------------
 __device__ __forceinline__ void ktab_tile(const SysDesc& d) {
   const Geom& g = d.g;
   const int ntot = g.nx + g.ny + g.nz;
   for (int i = threadIdx.x; i < ntot; i += kThreads) {
-    int n, k;
+    int n, k, ax;
     double r;
-    if (i < g.nx) { n = g.nx; k = i; r = d.rxd; }
-    else if (i < g.nx + g.ny) { n = g.ny; k = i - g.nx; r = d.ryd; }
-    else { n = g.nz; k = i - g.nx - g.ny; r = d.rzd; }
+    if (i < g.nx) { n = g.nx; k = i; r = d.rxd; ax = 0; }
+    else if (i < g.nx + g.ny) { n = g.ny; k = i - g.nx; r = d.ryd; ax = 1; }
+    else { n = g.nz; k = i - g.nx - g.ny; r = d.rzd; ax = 2; }
     const int nf = (n >> 1) + (n & 1);
     const int m = k < nf ? k : k - n;
-    const double mh = r * (double)m;
-    d.ktab[i] = mh;
-    d.ktab[ntot + i] = d.bmod[i] * exp(-d.fac * mh * mh);
+    if (!g.tric) {
+      const double mh = r * (double)m;
+      d.ktab[i] = mh;
+      d.ktab[ntot + i] = d.bmod[i] * exp(-d.fac * mh * mh);
+    } else {
+      const double md = (double)m;
+      d.ktab[i] = d.rm[ax] * md;
+      d.ktab[ntot + i] = d.bmod[i] * exp(-d.fac * d.gdiag[ax] * md * md);
+      d.ktab[2 * ntot + i] = d.rm[3 + ax] * md;
+      d.ktab[3 * ntot + i] = d.rm[6 + ax] * md;
+    }
   }
 }
 
@@ -306,35 +320,113 @@ __device__ __forceinline__ void ktab_tile(const SysDesc& d) {
 // even in m); its off-diagonal products m_i m_j change sign unless one of the two components sits
 // at k = 0 or on an even-length Nyquist plane, where the mirrored index maps onto itself.
 // Influence-table view for one tile: the tile's fixed kx values in registers, the y and z tables
-// staged in shared memory, all rounded once from the FP64 tables to FP32.
+// staged in shared memory, all rounded once from the FP64 tables to FP32.  Triclinic boxes stage
+// two more table rows (the k_y and k_z contributions) at my/mz + 2 (ny + nz) and + 3 (ny + nz).
 struct KTab {
   float m1, A1;
+  float m1b, m1c;    // triclinic: k_y and k_z contributions of kx
   const float* my;   // [ny] mhat_y
   const float* mz;   // [nz] mhat_z
   const float* Ay;   // [ny] A_y
   const float* Az;   // [nz] A_z
 };
 
-__host__ __device__ inline size_t ktab_smem_bytes(int ny, int nz) { return 2 * sizeof(float) * ((size_t)ny + nz); }
+__host__ __device__ inline size_t ktab_smem_bytes(int ny, int nz) { return 4 * sizeof(float) * ((size_t)ny + nz); }
 
-// Stage mhat and A for y and z into `sm` (2 (ny + nz) floats) and load kx's.  The caller
+// Stage mhat and A for y and z into `sm` (4 (ny + nz) floats) and load kx's.  The caller
 // synchronises before use.
 __device__ __forceinline__ KTab stage_ktab(const SysDesc& d, int kx, float* sm) {
   const Geom& g = d.g;
   const int ntot = g.nx + g.ny + g.nz;
   const int nyz = g.ny + g.nz;
-  for (int i = threadIdx.x; i < nyz; i += kThreads) {
-    sm[i] = (float)__ldcg(&d.ktab[g.nx + i]);
-    sm[nyz + i] = (float)__ldcg(&d.ktab[ntot + g.nx + i]);
+  const int rows = g.tric ? 4 : 2;
+  for (int i = threadIdx.x; i < rows * nyz; i += kThreads) {
+    const int r = i / nyz, j = i - r * nyz;
+    sm[i] = (float)__ldcg(&d.ktab[r * ntot + g.nx + j]);
   }
   KTab t;
   t.m1 = (float)__ldcg(&d.ktab[kx]);
   t.A1 = (float)__ldcg(&d.ktab[ntot + kx]);
+  t.m1b = g.tric ? (float)__ldcg(&d.ktab[2 * ntot + kx]) : 0.0f;
+  t.m1c = g.tric ? (float)__ldcg(&d.ktab[3 * ntot + kx]) : 0.0f;
   t.my = sm;
   t.mz = sm + g.ny;
   t.Ay = sm + nyz;
   t.Az = sm + nyz + g.ny;
   return t;
+}
+
+// Energy and virial terms of one k vector with weight w (1, or 2 for a stored element and its
+// mirror): t = w eterm |Q|^2 2^32, v = 2 (fac + 1/|k|^2); [t, t (v k0 k0 - 1), t v k0 k1, t v k0 k2,
+// t (v k1 k1 - 1), t v k1 k2, t (v k2 k2 - 1)], each rounded once to an integer.
+__device__ __forceinline__ void add_ev_terms(long long* acc, float eterm, float q2, float inv_msq,
+                                             float fac, float w, float k0, float k1, float k2) {
+  const float wt = __fmul_rn(w, __fmul_rn(__fmul_rn(eterm, q2), (float)kEvScale));
+  const float vt = __fmul_rn(2.0f, __fadd_rn(fac, inv_msq));
+  const float tv = __fmul_rn(wt, vt);
+  acc[0] += __float2ll_rn(wt);
+  acc[1] += __float2ll_rn(__fmul_rn(wt, __fmaf_rn(__fmul_rn(vt, k0), k0, -1.0f)));
+  acc[2] += __float2ll_rn(__fmul_rn(__fmul_rn(tv, k0), k1));
+  acc[3] += __float2ll_rn(__fmul_rn(__fmul_rn(tv, k0), k2));
+  acc[4] += __float2ll_rn(__fmul_rn(wt, __fmaf_rn(__fmul_rn(vt, k1), k1, -1.0f)));
+  acc[5] += __float2ll_rn(__fmul_rn(__fmul_rn(tv, k1), k2));
+  acc[6] += __float2ll_rn(__fmul_rn(wt, __fmaf_rn(__fmul_rn(vt, k2), k2, -1.0f)));
+}
+
+// Triclinic eterm of Miller indices (mx, my, mz) with k vector (k0, k1, k2) and per-axis product
+// a = piv_inv A_x A_y A_z: a exp(cross) / |k|^2.
+__device__ __forceinline__ float tric_eterm(const SysDesc& d, float a, float mx, float my, float mz,
+                                            float k0, float k1, float k2, float& inv_msq) {
+  inv_msq = __frcp_rn(__fmaf_rn(k2, k2, __fmaf_rn(k1, k1, __fmul_rn(k0, k0))));
+  const float arg = __fmaf_rn(d.cross_f[2], __fmul_rn(my, mz),
+                              __fmaf_rn(d.cross_f[1], __fmul_rn(mx, mz), __fmul_rn(d.cross_f[0], __fmul_rn(mx, my))));
+  return __fmul_rn(__fmul_rn(a, expf(arg)), inv_msq);
+}
+
+__device__ __forceinline__ float signed_index(int k, int n) {
+  return (float)(k < (n >> 1) + (n & 1) ? k : k - n);
+}
+
+// Triclinic solve of one stored element.  The x-mirror (kx >= 1) is the grid element
+// (nx - kx, ny - ky, nz - kz) with its own Miller indices, as for orthorhombic boxes: m' = -m unless
+// a component sits on an even-length Nyquist plane (or at 0), where m'_d = m_d.  When no component
+// is on a Nyquist plane k' = -k, with the same eterm and virial products, so the element counts
+// twice; otherwise the mirror's eterm and k' are evaluated separately.
+__device__ __forceinline__ void solve_elem_tric(float2& q, int kx, int ky, int kz, const SysDesc& d,
+                                                const KTab& kt, long long* acc) {
+  const Geom& g = d.g;
+  if (kx == 0 && ky == 0 && kz == 0) {
+    q = make_float2(0.0f, 0.0f);
+    return;
+  }
+  const int r2 = 2 * (g.ny + g.nz), r3 = 3 * (g.ny + g.nz);
+  const float cy0 = kt.my[ky], cy1 = kt.my[r2 + ky], cy2 = kt.my[r3 + ky];
+  const float cz0 = kt.mz[kz], cz1 = kt.mz[r2 + kz], cz2 = kt.mz[r3 + kz];
+  const float k0 = __fadd_rn(__fadd_rn(kt.m1, cy0), cz0);
+  const float k1 = __fadd_rn(__fadd_rn(kt.m1b, cy1), cz1);
+  const float k2 = __fadd_rn(__fadd_rn(kt.m1c, cy2), cz2);
+  const float mx = signed_index(kx, g.nx), my = signed_index(ky, g.ny), mz = signed_index(kz, g.nz);
+  const float a = __fmul_rn(__fmul_rn(__fmul_rn(d.piv_inv_f, kt.A1), kt.Ay[ky]), kt.Az[kz]);
+  float inv_msq;
+  const float eterm = tric_eterm(d, a, mx, my, mz, k0, k1, k2, inv_msq);
+  if (d.calc_ev) {
+    const float q2 = __fmaf_rn(q.y, q.y, __fmul_rn(q.x, q.x));
+    const bool nyq = (2 * kx == g.nx) || (2 * ky == g.ny) || (2 * kz == g.nz);
+    add_ev_terms(acc, eterm, q2, inv_msq, d.fac_f, (kx >= 1 && !nyq) ? 2.0f : 1.0f, k0, k1, k2);
+    if (kx >= 1 && nyq) {
+      const float sx = (2 * kx == g.nx) ? 1.0f : -1.0f;
+      const float sy = (ky == 0 || 2 * ky == g.ny) ? 1.0f : -1.0f;
+      const float sz = (kz == 0 || 2 * kz == g.nz) ? 1.0f : -1.0f;
+      const float j0 = __fadd_rn(__fadd_rn(sx * kt.m1, sy * cy0), sz * cz0);
+      const float j1 = __fadd_rn(__fadd_rn(sx * kt.m1b, sy * cy1), sz * cz1);
+      const float j2 = __fadd_rn(__fadd_rn(sx * kt.m1c, sy * cy2), sz * cz2);
+      float inv_msq_m;
+      const float eterm_m = tric_eterm(d, a, sx * mx, sy * my, sz * mz, j0, j1, j2, inv_msq_m);
+      add_ev_terms(acc, eterm_m, q2, inv_msq_m, d.fac_f, 1.0f, j0, j1, j2);
+    }
+  }
+  q.x = __fmul_rn(q.x, eterm);
+  q.y = __fmul_rn(q.y, eterm);
 }
 
 // Solve one stored element: Q *= eterm (Q(0) = 0) and, when asked, add its energy and virial
@@ -348,6 +440,10 @@ __device__ __forceinline__ KTab stage_ktab(const SysDesc& d, int kx, float* sm) 
 __device__ __forceinline__ void solve_elem(float2& q, int kx, int ky, int kz, const SysDesc& d,
                                            const KTab& kt, long long* acc) {
   const Geom& g = d.g;
+  if (g.tric) {
+    solve_elem_tric(q, kx, ky, kz, d, kt, acc);
+    return;
+  }
   if (kx == 0 && ky == 0 && kz == 0) {
     q = make_float2(0.0f, 0.0f);
     return;
@@ -488,7 +584,7 @@ __device__ __forceinline__ void z_tile(const SysDesc& d, int mode, int tile, flo
 // y inverse, all in shared memory (plane held as buf[z * (ny+1) + y]).  Used when the plane fits.
 __host__ __device__ inline size_t plane_smem_bytes(int ny, int nz) {
   return sizeof(float2) * ((size_t)ny + nz + 2 * (size_t)nz * (ny + 1)) + 32 * 7 * sizeof(long long) +
-         2 * sizeof(float) * ((size_t)ny + nz);
+         4 * sizeof(float) * ((size_t)ny + nz);
 }
 
 __device__ __forceinline__ void plane_tile(const SysDesc& d, int kx, float2* smem) {
@@ -573,9 +669,7 @@ __device__ __forceinline__ void bin_tile_p(const SysDesc& d, int tile, int parit
   for (int k = 0; k < NW; k++) w[k] = 0.0f;
   if (valid) {
     const float4 a = __ldg(&d.xyzq[i]);
-    frac_coord(a.x, g.sx_hi, g.sx_lo, g.nx, ix, ux);
-    frac_coord(a.y, g.sy_hi, g.sy_lo, g.ny, iy, uy);
-    frac_coord(a.z, g.sz_hi, g.sz_lo, g.nz, iz, uz);
+    frac_coords(g, a.x, a.y, a.z, ix, iy, iz, ux, uy, uz);
     bspline<P>(ux, w, nullptr);
 #pragma unroll
     for (int k = 0; k < P; k++) w[k] = __fmul_rn(a.w, w[k]);
@@ -1133,9 +1227,17 @@ __device__ __forceinline__ void gather_core(const SysDesc& d, int atom, bool val
   }
   if (valid && gl == 0) {
     const float qc = q * (float)kCcelec;
-    const float fx = qc * g.sx_hi * f.x;
-    const float fy = qc * g.sy_hi * f.y;
-    const float fz = qc * g.sz_hi * f.z;
+    float fx, fy, fz;
+    if (!g.tric) {
+      fx = qc * g.sx_hi * f.x;
+      fy = qc * g.sy_hi * f.y;
+      fz = qc * g.sz_hi * f.z;
+    } else {   // F_j = q ccelec sum_d R[j][d] n_d f_d
+      const float* S = g.shi;
+      fx = __fmul_rn(qc, __fmaf_rn(S[2], f.z, __fmaf_rn(S[1], f.y, __fmul_rn(S[0], f.x))));
+      fy = __fmul_rn(qc, __fmaf_rn(S[5], f.z, __fmaf_rn(S[4], f.y, __fmul_rn(S[3], f.x))));
+      fz = __fmul_rn(qc, __fmaf_rn(S[8], f.z, __fmaf_rn(S[7], f.y, __fmul_rn(S[6], f.x))));
+    }
     const size_t st = (size_t)d.stride;
     if (KIND == kForceF32Soa) {
       float* fo = (float*)d.force;
@@ -1161,9 +1263,7 @@ __device__ __forceinline__ void gather_atom(const SysDesc& d, int atom, bool val
   const float4 a = valid ? __ldg(&d.xyzq[atom]) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
   int ix, iy, iz;
   float ux, uy, uz;
-  frac_coord(a.x, g.sx_hi, g.sx_lo, g.nx, ix, ux);
-  frac_coord(a.y, g.sy_hi, g.sy_lo, g.ny, iy, uy);
-  frac_coord(a.z, g.sz_hi, g.sz_lo, g.nz, iz, uz);
+  frac_coords(g, a.x, a.y, a.z, ix, iy, iz, ux, uy, uz);
   gather_core<P, KIND, LPA>(d, atom, valid, gl, ix, iy, iz, ux, uy, uz, a.w);
 }
 

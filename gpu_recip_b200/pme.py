@@ -32,6 +32,16 @@ def recip_from_box(box: Sequence[float]) -> list:
     return [1.0 / bx, 0.0, 0.0, 0.0, 1.0 / by, 0.0, 0.0, 0.0, 1.0 / bz]
 
 
+def recip_from_box_vectors(vectors) -> list:
+    """Row-major reciprocal matrix R[j][d] (recip[3 j + d]) of a box whose vectors a, b, c are the
+    rows of ``vectors``: R is the inverse of that matrix, so the fractional coordinate along d is
+    sum_j x_j R[j][d].  A diagonal result is the orthorhombic case."""
+    B = np.asarray(vectors, dtype=np.float64).reshape(3, 3)
+    if not np.all(np.isfinite(B)) or abs(np.linalg.det(B)) == 0.0:
+        raise ValueError("box vectors must be finite and span a volume")
+    return [float(v) for v in np.linalg.inv(B).reshape(-1)]
+
+
 def force_stride(n: int, itemsize: int = 4) -> int:
     """SoA force stride padded to 256 bytes, as Force<T> (Force.h:63-69)."""
     return ((((n - 1 + 32) * itemsize) - 1) // 256 + 1) * 256 // itemsize
@@ -207,6 +217,15 @@ class CudaPMERecip:
                 "calc_self_energy")
 
     # -- fused evaluation (CudaDomdecRecip::calc) -----------------------------------------------
+    def eval(self, recip, xyzq, ncoord: int, kappa: float, calc_energy: bool, calc_virial: bool,
+             force, stride: int = 0, kind: Optional[int] = None):
+        """Fused evaluation for any box (pme_eval): recip is the row-major reciprocal matrix,
+        orthorhombic (diagonal) or triclinic."""
+        k = self._force_kind(force, stride) if kind is None else kind
+        C.check(self._lib.pme_eval(self._h, C.dbl9(recip), _xyzq_ptr(xyzq, ncoord), ncoord,
+                                   float(kappa), int(calc_energy), int(calc_virial), k, _ptr(force),
+                                   int(stride)), "eval")
+
     def eval_ortho(self, inv_box, xyzq, ncoord: int, kappa: float, calc_energy: bool,
                    calc_virial: bool, force, stride: int = 0, kind: Optional[int] = None):
         k = self._force_kind(force, stride) if kind is None else kind

@@ -24,6 +24,43 @@ def water_box(n_waters: int, box: Sequence[float], seed: int) -> np.ndarray:
     rng = np.random.default_rng(seed)
     box = np.asarray(box, dtype=np.float64).reshape(3)
     o = rng.random((n_waters, 3)) * box
+    h = _hydrogens(rng, o)
+    out = np.empty((n_waters, 3, 4))
+    out[:, 0, :3] = o
+    out[:, 1:, :3] = h
+    out[:, :, :3] = np.mod(out[:, :, :3], box)
+    out[:, 0, 3] = Q_O
+    out[:, 1:, 3] = Q_H
+    out = out.reshape(-1, 4).astype(np.float32)
+    # float32 rounding of a coordinate just below L can give exactly L: fold it back to 0
+    for d in range(3):
+        col = out[:, d]
+        col[col >= np.float32(box[d])] = 0.0
+    return out
+
+
+def water_cell(n_waters: int, vectors, seed: int) -> np.ndarray:
+    """Waters in a triclinic cell whose box vectors are the rows of ``vectors``: oxygens uniform in
+    the cell (uniform fractional coordinates), orientations as water_box, every atom wrapped into
+    the cell (fractional coordinates in [0, 1)).  (3*n_waters, 4) float32 xyzq."""
+    rng = np.random.default_rng(seed)
+    B = np.asarray(vectors, dtype=np.float64).reshape(3, 3)
+    R = np.linalg.inv(B)
+    o = rng.random((n_waters, 3)) @ B
+    h = _hydrogens(rng, o)
+    xyz = np.concatenate([o[:, None, :], h], axis=1).reshape(-1, 3)
+    frac = xyz @ R
+    frac -= np.floor(frac)
+    out = np.empty((3 * n_waters, 4))
+    out[:, :3] = frac @ B
+    out[:, 3] = np.tile([Q_O, Q_H, Q_H], n_waters)
+    return out.astype(np.float32)
+
+
+def _hydrogens(rng, o: np.ndarray) -> np.ndarray:
+    """(n, 2, 3) hydrogen positions of waters with oxygens at ``o`` and uniform random orientations
+    (unit quaternions from ``rng``)."""
+    n_waters = o.shape[0]
     q = rng.normal(size=(n_waters, 4))
     q /= np.linalg.norm(q, axis=1, keepdims=True)
     w, x, y, z = q[:, 0], q[:, 1], q[:, 2], q[:, 3]
@@ -40,19 +77,7 @@ def water_box(n_waters: int, box: Sequence[float], seed: int) -> np.ndarray:
     half = math.radians(ANGLE_HOH) / 2
     body = np.array([[R_OH * math.sin(half), R_OH * math.cos(half), 0.0],
                      [-R_OH * math.sin(half), R_OH * math.cos(half), 0.0]])
-    h = o[:, None, :] + np.einsum("nij,kj->nki", rot, body)
-    out = np.empty((n_waters, 3, 4))
-    out[:, 0, :3] = o
-    out[:, 1:, :3] = h
-    out[:, :, :3] = np.mod(out[:, :, :3], box)
-    out[:, 0, 3] = Q_O
-    out[:, 1:, 3] = Q_H
-    out = out.reshape(-1, 4).astype(np.float32)
-    # float32 rounding of a coordinate just below L can give exactly L: fold it back to 0
-    for d in range(3):
-        col = out[:, d]
-        col[col >= np.float32(box[d])] = 0.0
-    return out
+    return o[:, None, :] + np.einsum("nij,kj->nki", rot, body)
 
 
 def smooth235(lo: int, hi: int) -> List[int]:
@@ -75,6 +100,14 @@ class PmeSystem:
     nfft: tuple
     order: int
     kappa: float
+    vectors: tuple = None     # triclinic box vectors (rows); None for the orthorhombic `box`
+
+    @property
+    def recip9(self) -> list:
+        """Row-major reciprocal matrix R[j][d] (the inverse of the box-vector matrix)."""
+        if self.vectors is None:
+            return [1.0 / self.box[0], 0.0, 0.0, 0.0, 1.0 / self.box[1], 0.0, 0.0, 0.0, 1.0 / self.box[2]]
+        return [float(v) for v in np.linalg.inv(np.asarray(self.vectors, dtype=np.float64)).reshape(-1)]
 
     @property
     def natom(self) -> int:
@@ -111,6 +144,24 @@ def config_large(seed: int = 3) -> PmeSystem:
     L = 216.0
     return PmeSystem("water336k_216_p6", water_box(336000, (L, L, L), seed), (L, L, L),
                      (216, 216, 216), 6, 0.30)
+
+
+def config_triclinic_small(order: int = 4, seed: int = 5) -> PmeSystem:
+    """1,000 waters (3,000 atoms) in a general triclinic cell a = (32, 0, 0), b = (6, 31, 0),
+    c = (-5, 7, 30.5) A (angles 77-101 deg, volume equal to a 31.2 A cube), 32^3, kappa 0.34."""
+    V = ((32.0, 0.0, 0.0), (6.0, 31.0, 0.0), (-5.0, 7.0, 30.5))
+    return PmeSystem(f"water1k_tric_32_p{order}", water_cell(1000, V, seed), (32.0, 31.0, 30.5),
+                     (32, 32, 32), order, 0.34, V)
+
+
+def config_triclinic(order: int = 4, seed: int = 6) -> PmeSystem:
+    """8,000 waters (24,000 atoms) in a rhombic dodecahedron (xy-square form: a = (L, 0, 0),
+    b = (0, L, 0), c = (L/2, L/2, L/sqrt 2), L = 69.73 A; the volume of the 62.1 A cube), 64^3,
+    order 4 or 6, kappa 0.32."""
+    L = 69.73
+    V = ((L, 0.0, 0.0), (0.0, L, 0.0), (L / 2, L / 2, L / math.sqrt(2.0)))
+    return PmeSystem(f"water8k_dodec_64_p{order}", water_cell(8000, V, seed), (L, L, L / math.sqrt(2.0)),
+                     (64, 64, 64), order, 0.32, V)
 
 
 def batch_systems(count: int = 256, seed: int = 4, order: int = 4, kappa: float = 0.32,

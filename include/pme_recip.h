@@ -32,7 +32,7 @@ typedef struct pme_recip pme_recip;      /* opaque operator instance */
 
 typedef enum {
   PME_OK = 0,
-  PME_EINVAL = -1,        /* bad argument (null pointer, size, order, non-orthorhombic box) */
+  PME_EINVAL = -1,        /* bad argument (null pointer, size, order, singular or non-finite box) */
   PME_EUNSUPPORTED = -2,  /* valid but not supported (grid length with a prime factor > 5) */
   PME_ECUDA = -3,         /* CUDA runtime error */
   PME_ETIMEOUT = -4,      /* a bounded wait gave up */
@@ -70,7 +70,11 @@ PME_API int pme_print_info(const pme_recip* h);                    /* to stdout 
 
 /* ---- stages (CudaPMERecip.h:180-197) ----
  * xyzq: device float4[ncoord] (x, y, z, q).  recip: HOST double[9], row-major 3x3 reciprocal
- * box; only orthorhombic boxes are accepted (off-diagonals must be 0, as the reference). */
+ * box R[j][d] = recip[3 j + d], the inverse of the matrix whose rows are the box vectors, so that
+ * the fractional coordinate along d is sum_j x_j R[j][d].  A diagonal recip is the reference's
+ * orthorhombic case (CudaPMERecip.cu:2042-2045) and must be positive; off-diagonals select the
+ * triclinic forms of spread, solve and gather (an extension: the reference exits on them), which
+ * need a finite, non-singular matrix.  Anything else returns PME_EINVAL. */
 PME_API int pme_spread_charge(pme_recip* h, const void* xyzq, int ncoord, const double* recip);
 PME_API int pme_r2c_fft(pme_recip* h);
 PME_API int pme_scalar_sum(pme_recip* h, const double* recip, double kappa, int calc_energy,
@@ -99,6 +103,11 @@ PME_API int pme_energy_virial_device_ptr(pme_recip* h, double** dev_ptr);
 PME_API int pme_eval_ortho(pme_recip* h, double inv_boxx, double inv_boxy, double inv_boxz,
                    const void* xyzq, int ncoord, double kappa, int calc_energy, int calc_virial,
                    int kind, void* force, int stride);
+/* The same for any box: recip as for pme_spread_charge (orthorhombic or triclinic).  With a
+ * diagonal recip it is pme_eval_ortho.  No counterpart in the reference, which only takes
+ * orthorhombic boxes (CudaDomdecRecip.h:20-23 builds a diagonal recip). */
+PME_API int pme_eval(pme_recip* h, const double* recip, const void* xyzq, int ncoord, double kappa,
+                   int calc_energy, int calc_virial, int kind, void* force, int stride);
 
 /* ---- grid read-back for parity checks (synchronise the stream; host outputs) ----
  * Layouts follow the reference: real grids [z][y][x]; half-complex grid [z][y][kx],

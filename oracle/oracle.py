@@ -59,10 +59,16 @@ def lib():
         L.orc_self_energy.restype = D
         L.orc_eval.argtypes = [P, I, P, I, I, I, I, D, P, P, P, P, I]
         L.orc_hardware_threads.argtypes = []
+        L.orc_spread_f64_tric.argtypes = [P, I, P, I, I, I, I, P, I]
+        L.orc_spread_fixed_tric.argtypes = [P, I, P, I, I, I, I, P, I]
+        L.orc_scalar_sum_tric.argtypes = [P, I, I, I, I, P, D, I, P, P, I]
+        L.orc_gather_tric.argtypes = [P, I, P, P, I, I, I, I, P, I]
+        L.orc_eval_tric.argtypes = [P, I, P, I, I, I, I, D, P, P, P, P, I]
         for name in ("orc_bspline", "orc_spread_f64", "orc_spread_fixed", "orc_fixed_to_float",
                      "orc_fft1d", "orc_dft1d", "orc_fft3d_r2c", "orc_fft3d_c2r",
                      "orc_bspline_moduli", "orc_scalar_sum", "orc_gather", "orc_eval",
-                     "orc_hardware_threads"):
+                     "orc_hardware_threads", "orc_spread_f64_tric", "orc_spread_fixed_tric",
+                     "orc_scalar_sum_tric", "orc_gather_tric", "orc_eval_tric"):
             if name not in ("orc_fixed_to_float",):
                 getattr(L, name).restype = I
         _lib = L
@@ -95,24 +101,38 @@ def bspline_moduli(order: int, n: int) -> np.ndarray:
     return out
 
 
+def _box(recip):
+    """(suffix, array): recip given as the reciprocal diagonal (3 values) or the row-major 3x3
+    reciprocal matrix (9 values); a diagonal matrix takes the orthorhombic functions, anything
+    else the triclinic (*_tric) ones."""
+    r = np.ascontiguousarray(recip, dtype=np.float64).reshape(-1)
+    if r.size == 3:
+        return "", r
+    if r.size != 9:
+        raise ValueError("recip must hold 3 (diagonal) or 9 (matrix) values")
+    if np.all(r[[1, 2, 3, 5, 6, 7]] == 0.0):
+        return "", np.ascontiguousarray(r[[0, 4, 8]])
+    return "_tric", r
+
+
 def spread_f64(xyzq, recip3, nfft, order, nthreads=0) -> np.ndarray:
     x = np.ascontiguousarray(xyzq, dtype=np.float64).reshape(-1, 4)
-    r = np.ascontiguousarray(recip3, dtype=np.float64)
+    sfx, r = _box(recip3)
     nx, ny, nz = nfft
     g = np.zeros((nz, ny, nx))
-    _check(lib().orc_spread_f64(_p(x), x.shape[0], _p(r), nx, ny, nz, order, _p(g), nthreads),
-           "spread_f64")
+    _check(getattr(lib(), "orc_spread_f64" + sfx)(_p(x), x.shape[0], _p(r), nx, ny, nz, order, _p(g),
+                                                   nthreads), "spread_f64")
     return g
 
 
 def spread_fixed(xyzq, recip3, nfft, order, nthreads=0) -> np.ndarray:
     """int64 fixed-point grid (scale 2^40) from the FP32 mirror of the GPU spreading."""
     x = np.ascontiguousarray(xyzq, dtype=np.float32).reshape(-1, 4)
-    r = np.ascontiguousarray(recip3, dtype=np.float64)
+    sfx, r = _box(recip3)
     nx, ny, nz = nfft
     g = np.zeros((nz, ny, nx), dtype=np.int64)
-    _check(lib().orc_spread_fixed(_p(x), x.shape[0], _p(r), nx, ny, nz, order, _p(g), nthreads),
-           "spread_fixed")
+    _check(getattr(lib(), "orc_spread_fixed" + sfx)(_p(x), x.shape[0], _p(r), nx, ny, nz, order, _p(g),
+                                                     nthreads), "spread_fixed")
     return g
 
 
@@ -158,11 +178,11 @@ def scalar_sum(half: np.ndarray, nx: int, order: int, recip3, kappa: float, calc
     """Returns (solved half grid, energy, virial 3x3)."""
     h = np.ascontiguousarray(half, dtype=np.complex128).copy()
     nz, ny, hx = h.shape
-    r = np.ascontiguousarray(recip3, dtype=np.float64)
+    sfx, r = _box(recip3)
     e = np.zeros(1)
     v = np.zeros(9)
-    _check(lib().orc_scalar_sum(_p(h), nx, ny, nz, order, _p(r), float(kappa), int(calc_ev),
-                                _p(e), _p(v), nthreads), "scalar_sum")
+    _check(getattr(lib(), "orc_scalar_sum" + sfx)(_p(h), nx, ny, nz, order, _p(r), float(kappa),
+                                                   int(calc_ev), _p(e), _p(v), nthreads), "scalar_sum")
     return h, float(e[0]), v.reshape(3, 3)
 
 
@@ -170,10 +190,10 @@ def gather(xyzq, grid: np.ndarray, recip3, order, nthreads=0) -> np.ndarray:
     x = np.ascontiguousarray(xyzq, dtype=np.float64).reshape(-1, 4)
     g = np.ascontiguousarray(grid, dtype=np.float64)
     nz, ny, nx = g.shape
-    r = np.ascontiguousarray(recip3, dtype=np.float64)
+    sfx, r = _box(recip3)
     f = np.zeros((x.shape[0], 3))
-    _check(lib().orc_gather(_p(x), x.shape[0], _p(g), _p(r), nx, ny, nz, order, _p(f), nthreads),
-           "gather")
+    _check(getattr(lib(), "orc_gather" + sfx)(_p(x), x.shape[0], _p(g), _p(r), nx, ny, nz, order, _p(f),
+                                               nthreads), "gather")
     return f
 
 
@@ -185,13 +205,13 @@ def self_energy(xyzq, kappa) -> float:
 def evaluate(xyzq, recip3, nfft, order, kappa, nthreads=0):
     """Full FP64 evaluation.  Returns dict(force (N,3), energy, energy_self, virial (3,3))."""
     x = np.ascontiguousarray(xyzq, dtype=np.float64).reshape(-1, 4)
-    r = np.ascontiguousarray(recip3, dtype=np.float64)
+    sfx, r = _box(recip3)
     nx, ny, nz = nfft
     f = np.zeros((x.shape[0], 3))
     e = np.zeros(1)
     es = np.zeros(1)
     v = np.zeros(9)
-    _check(lib().orc_eval(_p(x), x.shape[0], _p(r), nx, ny, nz, order, float(kappa), _p(f),
-                          _p(e), _p(es), _p(v), nthreads), "eval")
+    _check(getattr(lib(), "orc_eval" + sfx)(_p(x), x.shape[0], _p(r), nx, ny, nz, order, float(kappa),
+                                             _p(f), _p(e), _p(es), _p(v), nthreads), "eval")
     return {"force": f, "energy": float(e[0]), "energy_self": float(es[0]),
             "virial": v.reshape(3, 3)}

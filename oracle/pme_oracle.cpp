@@ -15,6 +15,8 @@
 //   * influence function, energy and virial ........... CudaPMERecip.cu:594-901, :1960-2040
 //   * force gather (gradient, CHARMM sign) ............. CudaPMERecip.cu:1031-1245
 //   * self energy ...................................... CudaPMERecip.cu:1252-1275, :2052-2061
+//   * triclinic boxes (*_tric): an extension beyond the reference, which accepts only
+//     orthorhombic recip (CudaPMERecip.cu:2042-2045); same algorithm with full-matrix maps
 //
 // Two spreading modes:
 //   * orc_spread_f64:   FP64 weights, FP64 grid (the tolerance reference);
@@ -144,19 +146,68 @@ static inline void frac_f64(double x, double r, int n, int* i0, double* u) {
 }
 
 // ---------------------------------------------------------------------------------------------
+// Triclinic boxes -- an extension: the reference accepts only orthorhombic recip
+// (CudaPMERecip.cu:2042-2045).  recip9[3 j + d] = R[j][d] is the inverse of the matrix whose rows
+// are the box vectors: fractional coordinate s_d = sum_j x_j R[j][d], k vector of Miller indices m
+// k_j = sum_d R[j][d] m_d, cell volume V = 1 / |det R|.  Everything else is the orthorhombic
+// algorithm with these two maps.
+// ---------------------------------------------------------------------------------------------
+static inline void frac_f64_tric(const double* x, const double* R, int d, int n, int* i0, double* u) {
+  const double sd = x[0] * R[d] + x[1] * R[3 + d] + x[2] * R[6 + d];
+  frac_f64(sd, 1.0, n, i0, u);
+}
+
+// FP32 mirror of the kernel's triclinic coordinate: float-float sum of the three products (each
+// split exactly with fmaf, leading parts summed by two Knuth two-sums), then the tail of frac_f32.
+static inline void frac_f32_tric(const float* x, const float* shi, const float* slo, int d, int n,
+                                 int* i0, float* u) {
+  const float p0 = x[0] * shi[d], p1 = x[1] * shi[3 + d], p2 = x[2] * shi[6 + d];
+  const float e0 = std::fmaf(x[0], slo[d], std::fmaf(x[0], shi[d], -p0));
+  const float e1 = std::fmaf(x[1], slo[3 + d], std::fmaf(x[1], shi[3 + d], -p1));
+  const float e2 = std::fmaf(x[2], slo[6 + d], std::fmaf(x[2], shi[6 + d], -p2));
+  const float s01 = p0 + p1;
+  const float b01 = s01 - p0;
+  const float t01 = (p0 - (s01 - b01)) + (p1 - b01);
+  float p = s01 + p2;
+  const float b2 = p - s01;
+  const float t2 = (s01 - (p - b2)) + (p2 - b2);
+  float e = ((e0 + e1) + e2) + (t01 + t2);
+  if (!(std::fabs(p) < 16777216.0f)) { p = 0.0f; e = 0.0f; }
+  const float fl = std::floor(p);
+  float f = p - fl;
+  int i = (int)fl + (n >> 1);
+  if (n & 1) f = f + 0.5f;
+  float v = f + e;
+  if (v >= 1.0f) { v = v - 1.0f; i += 1; }
+  if (v < 0.0f) { v = v + 1.0f; i -= 1; }
+  i %= n;
+  if (i < 0) i += n;
+  *i0 = i;
+  *u = v;
+}
+
+static inline double det3(const double* m) {
+  return m[0] * (m[4] * m[8] - m[5] * m[7]) - m[1] * (m[3] * m[8] - m[5] * m[6]) +
+         m[2] * (m[3] * m[7] - m[4] * m[6]);
+}
+
+// ---------------------------------------------------------------------------------------------
 // Spreading (CudaPMERecip.cu:479-580).  Q[i0x+a, i0y+b, i0z+c] += q thx[a] thy[b] thz[c],
 // indices mod n, grid layout x + nx*(y + ny*z).  Threads own z-planes so that each grid point
 // is summed by one thread in atom order (deterministic for any thread count).
 // ---------------------------------------------------------------------------------------------
-extern "C" int orc_spread_f64(const double* xyzq, int natom, const double* recip3,
-                              int nx, int ny, int nz, int p, double* grid, int nthreads) {
+// frac(i, ix, iy, iz, ux, uy, uz): stencil origins and offsets of atom i.
+template <class Frac>
+static int spread_f64_impl(const double* xyzq, int natom, int nx, int ny, int nz, int p, double* grid,
+                           int nthreads, Frac frac) {
   if (natom < 0 || nx < p || ny < p || nz < p || p < 2 || p > 16) return -1;
   const size_t G = (size_t)nx * ny * nz;
   std::fill(grid, grid + G, 0.0);
   std::vector<int> iz0(natom);
   for (int i = 0; i < natom; i++) {
-    double u;
-    frac_f64(xyzq[4 * i + 2], recip3[2], nz, &iz0[i], &u);
+    int ix, iy;
+    double ux, uy, uz;
+    frac(i, &ix, &iy, &iz0[i], &ux, &uy, &uz);
   }
   parallel_for(hw_threads(nthreads), nz, [&](int z) {
     double thx[16], thy[16], thz[16];
@@ -166,9 +217,7 @@ extern "C" int orc_spread_f64(const double* xyzq, int natom, const double* recip
       if (c >= p) continue;
       int ix, iy, izz;
       double ux, uy, uz;
-      frac_f64(xyzq[4 * i + 0], recip3[0], nx, &ix, &ux);
-      frac_f64(xyzq[4 * i + 1], recip3[1], ny, &iy, &uy);
-      frac_f64(xyzq[4 * i + 2], recip3[2], nz, &izz, &uz);
+      frac(i, &ix, &iy, &izz, &ux, &uy, &uz);
       bspline_f64(p, ux, thx, nullptr);
       bspline_f64(p, uy, thy, nullptr);
       bspline_f64(p, uz, thz, nullptr);
@@ -187,21 +236,40 @@ extern "C" int orc_spread_f64(const double* xyzq, int natom, const double* recip
   return 0;
 }
 
+extern "C" int orc_spread_f64(const double* xyzq, int natom, const double* recip3,
+                              int nx, int ny, int nz, int p, double* grid, int nthreads) {
+  return spread_f64_impl(xyzq, natom, nx, ny, nz, p, grid, nthreads,
+                         [&](int i, int* ix, int* iy, int* iz, double* ux, double* uy, double* uz) {
+                           frac_f64(xyzq[4 * i + 0], recip3[0], nx, ix, ux);
+                           frac_f64(xyzq[4 * i + 1], recip3[1], ny, iy, uy);
+                           frac_f64(xyzq[4 * i + 2], recip3[2], nz, iz, uz);
+                         });
+}
+
+extern "C" int orc_spread_f64_tric(const double* xyzq, int natom, const double* recip9,
+                                   int nx, int ny, int nz, int p, double* grid, int nthreads) {
+  return spread_f64_impl(xyzq, natom, nx, ny, nz, p, grid, nthreads,
+                         [&](int i, int* ix, int* iy, int* iz, double* ux, double* uy, double* uz) {
+                           const double* x = xyzq + 4 * i;
+                           frac_f64_tric(x, recip9, 0, nx, ix, ux);
+                           frac_f64_tric(x, recip9, 1, ny, iy, uy);
+                           frac_f64_tric(x, recip9, 2, nz, iz, uz);
+                         });
+}
+
 // Fixed-point spreading, FP32 mirror: each contribution is ((q*thx[a])*thy[b])*thz[c] in FP32,
 // scaled by 2^40 and rounded to nearest-even int64 (CudaPMERecip.cu:44-66 write_grid<long long>).
-extern "C" int orc_spread_fixed(const float* xyzq, int natom, const double* recip3,
-                                int nx, int ny, int nz, int p, int64_t* grid, int nthreads) {
+template <class Frac>
+static int spread_fixed_impl(const float* xyzq, int natom, int nx, int ny, int nz, int p, int64_t* grid,
+                             int nthreads, Frac frac) {
   if (natom < 0 || nx < p || ny < p || nz < p || p < 2 || p > 16) return -1;
   const size_t G = (size_t)nx * ny * nz;
   std::fill(grid, grid + G, (int64_t)0);
-  float shi[3], slo[3];
-  split_scale(recip3[0], nx, &shi[0], &slo[0]);
-  split_scale(recip3[1], ny, &shi[1], &slo[1]);
-  split_scale(recip3[2], nz, &shi[2], &slo[2]);
   std::vector<int> iz0(natom);
   for (int i = 0; i < natom; i++) {
-    float u;
-    frac_f32(xyzq[4 * i + 2], shi[2], slo[2], nz, &iz0[i], &u);
+    int ix, iy;
+    float ux, uy, uz;
+    frac(i, &ix, &iy, &iz0[i], &ux, &uy, &uz);
   }
   parallel_for(hw_threads(nthreads), nz, [&](int z) {
     float thx[16], thy[16], thz[16];
@@ -211,9 +279,7 @@ extern "C" int orc_spread_fixed(const float* xyzq, int natom, const double* reci
       if (c >= p) continue;
       int ix, iy, izz;
       float ux, uy, uz;
-      frac_f32(xyzq[4 * i + 0], shi[0], slo[0], nx, &ix, &ux);
-      frac_f32(xyzq[4 * i + 1], shi[1], slo[1], ny, &iy, &uy);
-      frac_f32(xyzq[4 * i + 2], shi[2], slo[2], nz, &izz, &uz);
+      frac(i, &ix, &iy, &izz, &ux, &uy, &uz);
       bspline_f32(p, ux, thx);
       bspline_f32(p, uy, thy);
       bspline_f32(p, uz, thz);
@@ -231,6 +297,36 @@ extern "C" int orc_spread_fixed(const float* xyzq, int natom, const double* reci
     }
   });
   return 0;
+}
+
+extern "C" int orc_spread_fixed(const float* xyzq, int natom, const double* recip3,
+                                int nx, int ny, int nz, int p, int64_t* grid, int nthreads) {
+  float shi[3], slo[3];
+  split_scale(recip3[0], nx, &shi[0], &slo[0]);
+  split_scale(recip3[1], ny, &shi[1], &slo[1]);
+  split_scale(recip3[2], nz, &shi[2], &slo[2]);
+  return spread_fixed_impl(xyzq, natom, nx, ny, nz, p, grid, nthreads,
+                           [&](int i, int* ix, int* iy, int* iz, float* ux, float* uy, float* uz) {
+                             frac_f32(xyzq[4 * i + 0], shi[0], slo[0], nx, ix, ux);
+                             frac_f32(xyzq[4 * i + 1], shi[1], slo[1], ny, iy, uy);
+                             frac_f32(xyzq[4 * i + 2], shi[2], slo[2], nz, iz, uz);
+                           });
+}
+
+// Triclinic, FP32 mirror: S[j][d] = n_d R[j][d] split into float-float pairs.
+extern "C" int orc_spread_fixed_tric(const float* xyzq, int natom, const double* recip9,
+                                     int nx, int ny, int nz, int p, int64_t* grid, int nthreads) {
+  const int n3[3] = {nx, ny, nz};
+  float shi[9], slo[9];
+  for (int j = 0; j < 3; j++)
+    for (int d = 0; d < 3; d++) split_scale(recip9[3 * j + d], n3[d], &shi[3 * j + d], &slo[3 * j + d]);
+  return spread_fixed_impl(xyzq, natom, nx, ny, nz, p, grid, nthreads,
+                           [&](int i, int* ix, int* iy, int* iz, float* ux, float* uy, float* uz) {
+                             const float* x = xyzq + 4 * i;
+                             frac_f32_tric(x, shi, slo, 0, nx, ix, ux);
+                             frac_f32_tric(x, shi, slo, 1, ny, iy, uy);
+                             frac_f32_tric(x, shi, slo, 2, nz, iz, uz);
+                           });
 }
 
 // int64 fixed point -> FP32 grid value: the integer rounded once to float (round to nearest),
@@ -399,9 +495,10 @@ extern "C" int orc_bspline_moduli(int p, int n, double* bmod) {
 // doubles the Nyquist plane of an even nx).  energy = 1/2 ccelec sum, virial_ij =
 // -1/2 ccelec sum eterm |Q|^2 (2 (pi^2/kappa^2 + 1/m^2) m_i m_j - delta_ij).
 // ---------------------------------------------------------------------------------------------
-extern "C" int orc_scalar_sum(double* cgrid, int nx, int ny, int nz, int p, const double* recip3,
-                              double kappa, int calc_ev, double* energy, double* vir9,
-                              int nthreads) {
+// kvec(mx, my, mz, mh): k vector of the Miller indices; piv_inv = 1 / (pi V).
+template <class KVec>
+static int scalar_sum_impl(double* cgrid, int nx, int ny, int nz, int p, double piv_inv, double kappa,
+                           int calc_ev, double* energy, double* vir9, int nthreads, KVec kvec) {
   if (nx < 2 || ny < 2 || nz < 2 || kappa <= 0.0) return -1;
   std::vector<double> bx(nx), by(ny), bz(nz);
   if (orc_bspline_moduli(p, nx, bx.data()) || orc_bspline_moduli(p, ny, by.data()) ||
@@ -410,7 +507,6 @@ extern "C" int orc_scalar_sum(double* cgrid, int nx, int ny, int nz, int p, cons
   const int hx = nx / 2 + 1;
   const int nfx = nx / 2 + nx % 2, nfy = ny / 2 + ny % 2, nfz = nz / 2 + nz % 2;
   const double fac = kPi * kPi / (kappa * kappa);
-  const double piv_inv = recip3[0] * recip3[1] * recip3[2] / kPi;
   cplx* g = reinterpret_cast<cplx*>(cgrid);
   int T = hw_threads(nthreads);
   std::vector<double> part((size_t)nz * 7, 0.0);
@@ -418,7 +514,7 @@ extern "C" int orc_scalar_sum(double* cgrid, int nx, int ny, int nz, int p, cons
     int mx = kx < nfx ? kx : kx - nx;
     int my = ky < nfy ? ky : ky - ny;
     int mz = kz < nfz ? kz : kz - nz;
-    mh[0] = recip3[0] * mx; mh[1] = recip3[1] * my; mh[2] = recip3[2] * mz;
+    kvec(mx, my, mz, mh);
     double msq = mh[0] * mh[0] + mh[1] * mh[1] + mh[2] * mh[2];
     return std::exp(-fac * msq) * piv_inv * bx[kx] * by[ky] * bz[kz] / msq;
   };
@@ -470,20 +566,44 @@ extern "C" int orc_scalar_sum(double* cgrid, int nx, int ny, int nz, int p, cons
   return 0;
 }
 
+extern "C" int orc_scalar_sum(double* cgrid, int nx, int ny, int nz, int p, const double* recip3,
+                              double kappa, int calc_ev, double* energy, double* vir9,
+                              int nthreads) {
+  const double piv_inv = recip3[0] * recip3[1] * recip3[2] / kPi;
+  return scalar_sum_impl(cgrid, nx, ny, nz, p, piv_inv, kappa, calc_ev, energy, vir9, nthreads,
+                         [&](int mx, int my, int mz, double* mh) {
+                           mh[0] = recip3[0] * mx; mh[1] = recip3[1] * my; mh[2] = recip3[2] * mz;
+                         });
+}
+
+// Triclinic: k_j = sum_d R[j][d] m_d; the x-mirror is the grid element (nx-kx, ny-ky, nz-kz) with
+// its own Miller indices, as in the orthorhombic sum.
+extern "C" int orc_scalar_sum_tric(double* cgrid, int nx, int ny, int nz, int p, const double* recip9,
+                                   double kappa, int calc_ev, double* energy, double* vir9,
+                                   int nthreads) {
+  const double piv_inv = std::fabs(det3(recip9)) / kPi;
+  const double* R = recip9;
+  return scalar_sum_impl(cgrid, nx, ny, nz, p, piv_inv, kappa, calc_ev, energy, vir9, nthreads,
+                         [&](int mx, int my, int mz, double* mh) {
+                           for (int j = 0; j < 3; j++) mh[j] = R[3 * j] * mx + R[3 * j + 1] * my + R[3 * j + 2] * mz;
+                         });
+}
+
 // ---------------------------------------------------------------------------------------------
 // Gather (CudaPMERecip.cu:1031-1245).  F_d = q ccelec r_d n_d sum (dtheta_d theta theta) Phi,
 // i.e. +dE/dx (gradient; CHARMM convention).  Output AoS force[3*i + d].
 // ---------------------------------------------------------------------------------------------
-extern "C" int orc_gather(const double* xyzq, int natom, const double* grid, const double* recip3,
-                          int nx, int ny, int nz, int p, double* force, int nthreads) {
+// frac(i, ...) as for spreading; out(i, qc, f1, f2, f3) writes atom i's force from the three
+// grid-unit gradient sums.
+template <class Frac, class Out>
+static int gather_impl(const double* xyzq, int natom, const double* grid, int nx, int ny, int nz, int p,
+                       int nthreads, Frac frac, Out out) {
   if (natom < 0 || p < 2 || p > 16) return -1;
   parallel_for(hw_threads(nthreads), natom, [&](int i) {
     double thx[16], thy[16], thz[16], dx[16], dy[16], dz[16];
     int ix, iy, iz;
     double ux, uy, uz;
-    frac_f64(xyzq[4 * i + 0], recip3[0], nx, &ix, &ux);
-    frac_f64(xyzq[4 * i + 1], recip3[1], ny, &iy, &uy);
-    frac_f64(xyzq[4 * i + 2], recip3[2], nz, &iz, &uz);
+    frac(i, &ix, &iy, &iz, &ux, &uy, &uz);
     bspline_f64(p, ux, thx, dx);
     bspline_f64(p, uy, thy, dy);
     bspline_f64(p, uz, thz, dz);
@@ -502,12 +622,44 @@ extern "C" int orc_gather(const double* xyzq, int natom, const double* grid, con
         }
       }
     }
-    double qc = xyzq[4 * i + 3] * kCcelec;
-    force[3 * i + 0] = qc * recip3[0] * nx * f1;
-    force[3 * i + 1] = qc * recip3[1] * ny * f2;
-    force[3 * i + 2] = qc * recip3[2] * nz * f3;
+    out(i, xyzq[4 * i + 3] * kCcelec, f1, f2, f3);
   });
   return 0;
+}
+
+extern "C" int orc_gather(const double* xyzq, int natom, const double* grid, const double* recip3,
+                          int nx, int ny, int nz, int p, double* force, int nthreads) {
+  return gather_impl(
+      xyzq, natom, grid, nx, ny, nz, p, nthreads,
+      [&](int i, int* ix, int* iy, int* iz, double* ux, double* uy, double* uz) {
+        frac_f64(xyzq[4 * i + 0], recip3[0], nx, ix, ux);
+        frac_f64(xyzq[4 * i + 1], recip3[1], ny, iy, uy);
+        frac_f64(xyzq[4 * i + 2], recip3[2], nz, iz, uz);
+      },
+      [&](int i, double qc, double f1, double f2, double f3) {
+        force[3 * i + 0] = qc * recip3[0] * nx * f1;
+        force[3 * i + 1] = qc * recip3[1] * ny * f2;
+        force[3 * i + 2] = qc * recip3[2] * nz * f3;
+      });
+}
+
+// Triclinic: F_j = q ccelec sum_d R[j][d] n_d f_d (the chain rule through s_d = sum_j x_j R[j][d]).
+extern "C" int orc_gather_tric(const double* xyzq, int natom, const double* grid, const double* recip9,
+                               int nx, int ny, int nz, int p, double* force, int nthreads) {
+  const double* R = recip9;
+  return gather_impl(
+      xyzq, natom, grid, nx, ny, nz, p, nthreads,
+      [&](int i, int* ix, int* iy, int* iz, double* ux, double* uy, double* uz) {
+        const double* x = xyzq + 4 * i;
+        frac_f64_tric(x, R, 0, nx, ix, ux);
+        frac_f64_tric(x, R, 1, ny, iy, uy);
+        frac_f64_tric(x, R, 2, nz, iz, uz);
+      },
+      [&](int i, double qc, double f1, double f2, double f3) {
+        const double g0 = nx * f1, g1 = ny * f2, g2 = nz * f3;
+        for (int j = 0; j < 3; j++)
+          force[3 * i + j] = qc * (R[3 * j] * g0 + R[3 * j + 1] * g1 + R[3 * j + 2] * g2);
+      });
 }
 
 // Self energy (CudaPMERecip.cu:1252-1275): -kappa ccelec / sqrt(pi) * sum q^2.
@@ -535,6 +687,28 @@ extern "C" int orc_eval(const double* xyzq, int natom, const double* recip3, int
   if (rc) return rc;
   orc_fft3d_c2r(cg.data(), nx, ny, nz, grid.data(), nthreads);
   rc = orc_gather(xyzq, natom, grid.data(), recip3, nx, ny, nz, p, force, nthreads);
+  if (rc) return rc;
+  if (e_recip) *e_recip = e;
+  if (vir9) for (int i = 0; i < 9; i++) vir9[i] = v[i];
+  if (e_self) *e_self = orc_self_energy(xyzq, natom, kappa);
+  return 0;
+}
+
+// Whole triclinic evaluation in FP64 (recip9 as for orc_spread_f64_tric).
+extern "C" int orc_eval_tric(const double* xyzq, int natom, const double* recip9, int nx, int ny,
+                             int nz, int p, double kappa, double* force, double* e_recip,
+                             double* e_self, double* vir9, int nthreads) {
+  const size_t G = (size_t)nx * ny * nz;
+  const size_t H = (size_t)(nx / 2 + 1) * ny * nz;
+  std::vector<double> grid(G), cg(2 * H);
+  int rc = orc_spread_f64_tric(xyzq, natom, recip9, nx, ny, nz, p, grid.data(), nthreads);
+  if (rc) return rc;
+  orc_fft3d_r2c(grid.data(), nx, ny, nz, cg.data(), nthreads);
+  double e = 0.0, v[9] = {0};
+  rc = orc_scalar_sum_tric(cg.data(), nx, ny, nz, p, recip9, kappa, 1, &e, v, nthreads);
+  if (rc) return rc;
+  orc_fft3d_c2r(cg.data(), nx, ny, nz, grid.data(), nthreads);
+  rc = orc_gather_tric(xyzq, natom, grid.data(), recip9, nx, ny, nz, p, force, nthreads);
   if (rc) return rc;
   if (e_recip) *e_recip = e;
   if (vir9) for (int i = 0; i < 9; i++) vir9[i] = v[i];

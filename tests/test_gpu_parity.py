@@ -252,8 +252,11 @@ def test_invalid_arguments_rejected(cuda):
     assert e.value.status == _capi.PME_EUNSUPPORTED
     pme = CudaPMERecip(32, 32, 32, 4)
     x = cuda.zeros((4, 4), device="cuda")
-    with pytest.raises(_capi.PMEError) as e:
-        pme.spread_charge(x, 4, [0.1, 0.01, 0, 0, 0.1, 0, 0, 0, 0.1])
+    with pytest.raises(_capi.PMEError) as e:   # singular matrix (the first two rows are equal)
+        pme.spread_charge(x, 4, [0.1, 0.1, 0, 0.1, 0.1, 0, 0, 0, 0.1])
+    assert e.value.status == _capi.PME_EINVAL
+    with pytest.raises(_capi.PMEError) as e:   # negative diagonal of an orthorhombic box
+        pme.spread_charge(x, 4, [-0.1, 0, 0, 0, 0.1, 0, 0, 0, 0.1])
     assert e.value.status == _capi.PME_EINVAL
 
 
