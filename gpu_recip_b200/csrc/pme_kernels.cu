@@ -18,14 +18,23 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <map>
+#include <mutex>
+#include <utility>
+
 #include "pme_internal.h"
 #include "pme_tiles.cuh"
 
 namespace pme {
 
 // Copy a descriptor (kernel parameter or global table entry) into shared memory.
+// Copy a kernel's SysDesc parameter (a __grid_constant__, read in place from the parameter space)
+// into shared memory, one word per thread.
 __device__ __forceinline__ void load_desc(SysDesc& dst, const SysDesc& src_param) {
-  if (threadIdx.x == 0) dst = src_param;
+  const int n = (int)(sizeof(SysDesc) / sizeof(int));
+  const int* s = reinterpret_cast<const int*>(&src_param);
+  int* t = reinterpret_cast<int*>(&dst);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) t[i] = s[i];
   __syncthreads();
 }
 
@@ -38,14 +47,14 @@ __device__ __forceinline__ void load_desc_global(SysDesc& dst, const SysDesc* sr
 }
 
 // ------------------------------- staged kernels ----------------------------------------------
-__global__ void __launch_bounds__(kThreads) k_spread(SysDesc p) {
+__global__ void __launch_bounds__(kThreads) k_spread(const __grid_constant__ SysDesc p) {
   __shared__ SysDesc d;
   extern __shared__ float2 smem[];
   load_desc(d, p);
   spread_dispatch(d, blockIdx.x, smem);
 }
 
-__global__ void __launch_bounds__(kThreads) k_self(SysDesc p) {
+__global__ void __launch_bounds__(kThreads) k_self(const __grid_constant__ SysDesc p) {
   __shared__ SysDesc d;
   __shared__ long long red[32];
   load_desc(d, p);
@@ -56,47 +65,47 @@ __global__ void __launch_bounds__(kThreads) k_self(SysDesc p) {
   if (threadIdx.x == 0 && sum != 0) atomicAdd((unsigned long long*)&d.acc[kAccQ2], (unsigned long long)sum);
 }
 
-__global__ void __launch_bounds__(kThreads) k_ktab(SysDesc p) {
+__global__ void __launch_bounds__(kThreads) k_ktab(const __grid_constant__ SysDesc p) {
   __shared__ SysDesc d;
   load_desc(d, p);
   ktab_tile(d);
 }
 
-__global__ void __launch_bounds__(kThreads) k_x_fwd(SysDesc p, int zero_accum) {
+__global__ void __launch_bounds__(kThreads) k_x_fwd(const __grid_constant__ SysDesc p, int zero_accum) {
   __shared__ SysDesc d;
   extern __shared__ float2 smem[];
   load_desc(d, p);
   x_fwd_tile(d, blockIdx.x, smem, zero_accum != 0);
 }
 
-__global__ void __launch_bounds__(kThreads) k_x_inv(SysDesc p) {
+__global__ void __launch_bounds__(kThreads) k_x_inv(const __grid_constant__ SysDesc p) {
   __shared__ SysDesc d;
   extern __shared__ float2 smem[];
   load_desc(d, p);
   x_inv_tile(d, blockIdx.x, smem);
 }
 
-__global__ void __launch_bounds__(kThreads) k_ypass(SysDesc p, int mode) {
+__global__ void __launch_bounds__(kThreads) k_ypass(const __grid_constant__ SysDesc p, int mode) {
   __shared__ SysDesc d;
   extern __shared__ float2 smem[];
   load_desc(d, p);
   y_tile(d, mode, blockIdx.x, smem);
 }
 
-__global__ void __launch_bounds__(kThreads) k_zpass(SysDesc p, int mode) {
+__global__ void __launch_bounds__(kThreads) k_zpass(const __grid_constant__ SysDesc p, int mode) {
   __shared__ SysDesc d;
   extern __shared__ float2 smem[];
   load_desc(d, p);
   z_tile(d, mode, blockIdx.x, smem);
 }
 
-__global__ void __launch_bounds__(kThreads) k_gather(SysDesc p) {
+__global__ void __launch_bounds__(kThreads) k_gather(const __grid_constant__ SysDesc p) {
   __shared__ SysDesc d;
   load_desc(d, p);
   gather_dispatch(d, blockIdx.x);
 }
 
-__global__ void k_finalize(SysDesc p, int solve, int self) {
+__global__ void k_finalize(const __grid_constant__ SysDesc p, int solve, int self) {
   if (threadIdx.x == 0 && blockIdx.x == 0) finalize_system(p, solve != 0, self != 0);
 }
 
@@ -250,8 +259,8 @@ __device__ __forceinline__ void fused_body(const FusedArgs& a) {
 // tile per CTA in a phase.  Throughput build: at most 80 registers, 3 CTAs per SM (a few spills in
 // the largest tiles); for launches with many tiles per CTA, where the extra resident warps hide
 // more latency than the spills cost.
-__global__ void __launch_bounds__(kThreads) k_fused_lat(FusedArgs a) { fused_body(a); }
-__global__ void __launch_bounds__(kThreads, 3) k_fused_tput(FusedArgs a) { fused_body(a); }
+__global__ void __launch_bounds__(kThreads) k_fused_lat(const __grid_constant__ FusedArgs a) { fused_body(a); }
+__global__ void __launch_bounds__(kThreads, 3) k_fused_tput(const __grid_constant__ FusedArgs a) { fused_body(a); }
 
 // ------------------------------- host launchers ----------------------------------------------
 static size_t staged_fft_smem(int L, int tx) { return tile_smem_bytes(L, tx) + 32 * 7 * sizeof(long long); }
@@ -351,15 +360,43 @@ static const void* fused_kernel(int variant) {
   return variant == kFusedThroughput ? (const void*)k_fused_tput : (const void*)k_fused_lat;
 }
 
-cudaError_t fused_shape(const int* total, size_t smem, int grid_cap, FusedShape* out) {
-  int dev = 0, sms = 0, occ_lat = 0, occ_tput = 0;
+// Resident CTAs per SM of the two builds at a dynamic shared-memory size, and the SM count, per
+// device (the occupancy queries cost host time on every launch-shape choice otherwise).
+struct Occupancy {
+  int sms, lat, tput;
+};
+
+static cudaError_t occupancy(size_t smem, Occupancy* out) {
+  static std::mutex mu;
+  static std::map<std::pair<int, size_t>, Occupancy> cache;
+  int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
-  if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
-  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_lat, k_fused_lat, kThreads, smem)) != cudaSuccess)
+  {
+    std::lock_guard<std::mutex> g(mu);
+    auto it = cache.find({dev, smem});
+    if (it != cache.end()) {
+      *out = it->second;
+      return cudaSuccess;
+    }
+  }
+  Occupancy o;
+  if ((e = cudaDeviceGetAttribute(&o.sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o.lat, k_fused_lat, kThreads, smem)) != cudaSuccess)
     return e;
-  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_tput, k_fused_tput, kThreads, smem)) != cudaSuccess)
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o.tput, k_fused_tput, kThreads, smem)) != cudaSuccess)
     return e;
+  std::lock_guard<std::mutex> g(mu);
+  cache[{dev, smem}] = o;
+  *out = o;
+  return cudaSuccess;
+}
+
+cudaError_t fused_shape(const int* total, size_t smem, int grid_cap, FusedShape* out) {
+  Occupancy o;
+  cudaError_t e = occupancy(smem, &o);
+  if (e != cudaSuccess) return e;
+  const int sms = o.sms, occ_lat = o.lat, occ_tput = o.tput;
   int most = 1;
   for (int p = 0; p < kPhases; p++) most = most > total[p] ? most : total[p];
   // many tiles per CTA: more resident CTAs pay; about one: fewer registers per thread cost

@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -150,6 +151,8 @@ struct Request {
   double t_submit = 0, t_admit = 0, t_done = 0;
   // host: pinned staging of the coordinates and of the results
   float* h_stage = nullptr;   // [natom*4 xyzq][n_evals*kEvCount doubles][natom*3 force]
+  size_t stage_cap = 0;       // bytes of the h_stage buffer (a pooled buffer may be larger)
+  bool stage_in_arena = false;   // h_stage is a block of the server's pinned host arena
   // device
   size_t off = 0, bytes = 0;
   SystemState st;
@@ -200,6 +203,11 @@ int check_request(const pme_request* q) {
 
 }  // namespace
 
+struct HostTables {
+  std::vector<float2> tw;
+  std::vector<double> bmod;
+};
+
 struct pme_server {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -238,11 +246,79 @@ struct pme_server {
   bool stop = false;
   bool failed = false;
   std::thread worker;
+  // pinned staging buffers and completion events of finished requests, reused by later ones:
+  // cudaHostAlloc is slow, and cudaFreeHost can synchronise the device under running steps
+  char* h_arena = nullptr;                    // pinned host arena for request staging
+  Arena harena;
+  std::multimap<size_t, float*> stage_pool;   // capacity -> buffer (staging beyond the arena)
+  size_t stage_pool_bytes = 0;
+  std::vector<cudaEvent_t> event_pool;
+  // twiddles and B-spline moduli by (nx, ny, nz, order): built once on the host (the moduli are an
+  // O(n^2) sum per axis) and shared by every request of that grid
+  std::map<std::array<int, 4>, HostTables> tables;
+  const HostTables& tables_for(const SystemState& st) {
+    const std::array<int, 4> key = {st.nx, st.ny, st.nz, st.order};
+    auto it = tables.find(key);
+    if (it == tables.end()) {
+      HostTables t;
+      st.host_tables(t.tw, t.bmod);
+      it = tables.emplace(key, std::move(t)).first;
+    }
+    return it->second;
+  }
   // statistics
   long long n_submitted = 0, n_completed = 0, n_evals = 0, n_steps = 0;
 };
 
 namespace {
+
+constexpr size_t kHostArenaBytes = 256ull << 20;  // pinned staging arena (at most)
+constexpr size_t kStagePoolMax = 512ull << 20;   // pinned bytes kept for reuse beyond the arena
+
+// Take a pooled staging buffer of at least `need` bytes (at most twice that) and a pooled event,
+// if there are any (lock held).
+void take_staging(pme_server* s, Request* q, size_t need) {
+  size_t off = 0;
+  if (s->h_arena && s->harena.alloc(need, &off)) {
+    q->h_stage = (float*)(s->h_arena + off);
+    q->stage_cap = need;
+    q->stage_in_arena = true;
+  }
+  auto it = q->h_stage ? s->stage_pool.end() : s->stage_pool.lower_bound(need);
+  if (it != s->stage_pool.end() && it->first <= 2 * need + 65536) {
+    q->h_stage = it->second;
+    q->stage_cap = it->first;
+    s->stage_pool_bytes -= it->first;
+    s->stage_pool.erase(it);
+  }
+  if (!s->event_pool.empty()) {
+    q->done_ev = s->event_pool.back();
+    s->event_pool.pop_back();
+  }
+}
+
+// Return a request's staging buffer and event to the pools (lock held); buffers beyond the
+// pool's limit are freed.
+void release_staging(pme_server* s, Request* q) {
+  if (q->h_stage && q->stage_in_arena) {
+    s->harena.release((size_t)((char*)q->h_stage - s->h_arena), q->stage_cap);
+    q->h_stage = nullptr;
+    q->stage_in_arena = false;
+  }
+  if (q->h_stage) {
+    if (s->stage_pool_bytes + q->stage_cap <= kStagePoolMax) {
+      s->stage_pool.emplace(q->stage_cap, q->h_stage);
+      s->stage_pool_bytes += q->stage_cap;
+    } else {
+      cudaFreeHost(q->h_stage);
+    }
+    q->h_stage = nullptr;
+  }
+  if (q->done_ev) {
+    s->event_pool.push_back(q->done_ev);
+    q->done_ev = nullptr;
+  }
+}
 
 // Allocate, clear and fill the device state of a pending request (worker thread, lock held).
 int admit(pme_server* s, Request* q) {
@@ -266,9 +342,9 @@ int admit(pme_server* s, Request* q) {
   q->hist = (double*)(p + sys + bins + 2 * xb + fb);
   // twiddles, moduli and coordinates from the request's pinned staging copy (stream-ordered after
   // the clear)
-  std::vector<float2> twh;
-  std::vector<double> bm;
-  q->st.host_tables(twh, bm);
+  const HostTables& tab = s->tables_for(q->st);
+  const std::vector<float2>& twh = tab.tw;
+  const std::vector<double>& bm = tab.bmod;
   char* ht = q->h_tables();
   std::memcpy(ht, twh.data(), twh.size() * sizeof(float2));
   std::memcpy(ht + twh.size() * sizeof(float2), bm.data(), bm.size() * sizeof(double));
@@ -508,6 +584,14 @@ int pme_server_create(size_t device_bytes, int max_active, void* stream, pme_ser
   for (int i = 0; i < 2 && e == cudaSuccess; i++) e = cudaHostAlloc(&s->h_stage[i], table, cudaHostAllocDefault);
   if (e == cudaSuccess) e = cudaHostAlloc(&s->h_status, 2 * sizeof(int), cudaHostAllocDefault);
   if (e == cudaSuccess) s->h_status[0] = s->h_status[1] = kStatusOk;
+  // pinned staging of submitted requests comes from one arena allocated here, so that submit
+  // makes no pinned allocation (which holds the driver against the worker's launches); requests
+  // beyond it allocate their own
+  if (e == cudaSuccess) {
+    const size_t hb = std::min<size_t>(kHostArenaBytes, std::max<size_t>(device_bytes / 16, 16u << 20));
+    if (cudaHostAlloc(&s->h_arena, hb, cudaHostAllocDefault) == cudaSuccess) s->harena.reset(hb);
+    else { cudaGetLastError(); s->h_arena = nullptr; }
+  }
   if (e != cudaSuccess) {
     cudaGetLastError();
     cudaFree(s->d_arena);
@@ -542,18 +626,27 @@ int pme_server_submit(pme_server* s, const pme_request* r, long long* id) {
   if (!q) return fail(PME_ENOMEM, "host allocation failed");
   q->r = *r;
   q->bytes = bytes;
+  const size_t need = Request::stage_bytes(*r);
   cudaError_t e = cudaSetDevice(s->device);
-  if (e == cudaSuccess) e = cudaHostAlloc(&q->h_stage, Request::stage_bytes(*r), cudaHostAllocDefault);
-  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&q->done_ev, cudaEventDisableTiming);
+  {
+    std::lock_guard<std::mutex> lock(s->mu);
+    take_staging(s, q.get(), need);
+  }
+  if (e == cudaSuccess && !q->h_stage) {
+    q->stage_cap = (need + 4095) & ~(size_t)4095;
+    e = cudaHostAlloc(&q->h_stage, q->stage_cap, cudaHostAllocDefault);
+    if (e != cudaSuccess) q->h_stage = nullptr;
+  }
+  if (e == cudaSuccess && !q->done_ev) e = cudaEventCreateWithFlags(&q->done_ev, cudaEventDisableTiming);
   if (e != cudaSuccess) {
-    if (q->h_stage) cudaFreeHost(q->h_stage);
+    std::lock_guard<std::mutex> lock(s->mu);
+    release_staging(s, q.get());
     return cuda_fail(e, "server: request staging");
   }
   std::memcpy(q->h_stage, r->xyzq, (size_t)r->natom * 16);
   std::lock_guard<std::mutex> lock(s->mu);
   if (s->stop) {
-    cudaFreeHost(q->h_stage);
-    cudaEventDestroy(q->done_ev);
+    release_staging(s, q.get());
     return fail(PME_ESTATE, "server is shutting down");
   }
   q->id = s->next_id++;
@@ -585,8 +678,7 @@ int pme_server_wait(pme_server* s, long long id, double timeout_s, double* times
     times3[2] = q->t_done;
   }
   const int status = q->status;
-  cudaFreeHost(q->h_stage);
-  cudaEventDestroy(q->done_ev);
+  release_staging(s, q);
   s->reqs.erase(it);
   if (status != PME_OK) return fail(status, "request failed");
   return PME_OK;
@@ -618,9 +710,12 @@ int pme_server_destroy(pme_server* s) {
   cudaSetDevice(s->device);
   cudaStreamSynchronize(s->stream);
   for (auto& kv : s->reqs) {
-    if (kv.second->h_stage) cudaFreeHost(kv.second->h_stage);
+    if (kv.second->h_stage && !kv.second->stage_in_arena) cudaFreeHost(kv.second->h_stage);
     if (kv.second->done_ev) cudaEventDestroy(kv.second->done_ev);
   }
+  for (auto& kv : s->stage_pool) cudaFreeHost(kv.second);
+  if (s->h_arena) cudaFreeHost(s->h_arena);
+  for (cudaEvent_t ev : s->event_pool) cudaEventDestroy(ev);
   cudaFree(s->d_arena);
   cudaFree(s->d_table);
   cudaFree(s->d_bar);

@@ -440,10 +440,6 @@ __device__ __forceinline__ void solve_elem_tric(float2& q, int kx, int ky, int k
 __device__ __forceinline__ void solve_elem(float2& q, int kx, int ky, int kz, const SysDesc& d,
                                            const KTab& kt, long long* acc) {
   const Geom& g = d.g;
-  if (g.tric) {
-    solve_elem_tric(q, kx, ky, kz, d, kt, acc);
-    return;
-  }
   if (kx == 0 && ky == 0 && kz == 0) {
     q = make_float2(0.0f, 0.0f);
     return;
@@ -496,6 +492,22 @@ __device__ __forceinline__ void flush_ev(const SysDesc& d, long long (&acc)[7], 
     for (int w = 0; w < nw; w++) sum += red[w * 7 + threadIdx.x];
     atomicAdd((unsigned long long*)&d.acc[kAccE + threadIdx.x], (unsigned long long)sum);
   }
+}
+
+// Triclinic solve of a span of stored elements held in shared memory: element (a, b), a = i div w,
+// b = i - a w for i < count, at buf[a ld + b] with ky = y0 + b, kz = a (elements with b >= nb are
+// padding), then the block's energy/virial flush.  Out of line so that the orthorhombic z and
+// plane tiles keep their compact code (cold instruction fetch is part of a single evaluation's
+// latency).  Every thread of the CTA calls it.
+static __device__ __noinline__ void solve_span_tric(const SysDesc& d, float2* buf, int ld, int count, int w,
+                                                    FastDiv wd, int nb, int kx, int y0, const KTab kt,
+                                                    long long* red) {
+  long long acc[7] = {0, 0, 0, 0, 0, 0, 0};
+  for (int idx = threadIdx.x; idx < count; idx += kThreads) {
+    const int a = fdiv(idx, wd), b = idx - a * w;
+    if (b < nb) solve_elem_tric(buf[a * ld + b], kx, y0 + b, a, d, kt, acc);
+  }
+  if (d.calc_ev) flush_ev(d, acc, red);
 }
 
 // y pass: tx_y consecutive y-lines (line = kx nz + z, contiguous ny values).  mode 0 forward,
@@ -561,12 +573,16 @@ __device__ __forceinline__ void z_tile(const SysDesc& d, int mode, int tile, flo
   if (mode == 0 || mode == 2) res = fft_tile(b0, b1, plan, ld, 1, ln, tw, false);
   if (mode == 1) res = fft_tile(b0, b1, plan, ld, 1, ln, tw, true);
   if (mode == 2 || mode == 3) {
-    long long acc[7] = {0, 0, 0, 0, 0, 0, 0};
-    for (int idx = tid; idx < L * tx; idx += kThreads) {
-      const int e = fdiv(idx, txd), t = idx - e * tx;
-      if (t < nt) solve_elem(res[e * ld + t], kx, y0 + t, e, d, kt, acc);
+    if (g.tric) {
+      solve_span_tric(d, res, ld, L * tx, tx, txd, nt, kx, y0, kt, red);
+    } else {
+      long long acc[7] = {0, 0, 0, 0, 0, 0, 0};
+      for (int idx = tid; idx < L * tx; idx += kThreads) {
+        const int e = fdiv(idx, txd), t = idx - e * tx;
+        if (t < nt) solve_elem(res[e * ld + t], kx, y0 + t, e, d, kt, acc);
+      }
+      if (d.calc_ev) flush_ev(d, acc, red);
     }
-    if (d.calc_ev) flush_ev(d, acc, red);
     __syncthreads();
     if (mode == 2) {
       float2* other = (res == b0) ? b1 : b0;
@@ -617,12 +633,16 @@ __device__ __forceinline__ void plane_tile(const SysDesc& d, int kx, float2* sme
   float2* o = (r == b0) ? b1 : b0;
   r = fft_tile(r, o, d.pz, LD, 1, ly, twz, false);
   step_mark(d, 11);
-  long long acc[7] = {0, 0, 0, 0, 0, 0, 0};
-  for (int idx = tid; idx < ny * nz; idx += kThreads) {
-    const int z = fdiv(idx, nyd), y = idx - z * ny;
-    solve_elem(r[z * LD + y], kx, y, z, d, kt, acc);
+  if (g.tric) {
+    solve_span_tric(d, r, LD, ny * nz, ny, nyd, ny, kx, 0, kt, red);
+  } else {
+    long long acc[7] = {0, 0, 0, 0, 0, 0, 0};
+    for (int idx = tid; idx < ny * nz; idx += kThreads) {
+      const int z = fdiv(idx, nyd), y = idx - z * ny;
+      solve_elem(r[z * LD + y], kx, y, z, d, kt, acc);
+    }
+    if (d.calc_ev) flush_ev(d, acc, red);
   }
-  if (d.calc_ev) flush_ev(d, acc, red);
   __syncthreads();
   step_mark(d, 12);
   o = (r == b0) ? b1 : b0;
