@@ -64,6 +64,10 @@ def lib():
         L.orc_scalar_sum_tric.argtypes = [P, I, I, I, I, P, D, I, P, P, I]
         L.orc_gather_tric.argtypes = [P, I, P, P, I, I, I, I, P, I]
         L.orc_eval_tric.argtypes = [P, I, P, I, I, I, I, D, P, P, P, P, I]
+        L.orc_direct_force.argtypes = [P, I, P, D, D, P, P, P, P, P, P, P, P, I]
+        L.orc_direct_14.argtypes = [P, P, D, D, D, P, P, P, I, P, I, P, P, P, P, P]
+        for name in ("orc_direct_force", "orc_direct_14"):
+            getattr(L, name).restype = I
         for name in ("orc_bspline", "orc_spread_f64", "orc_spread_fixed", "orc_fixed_to_float",
                      "orc_fft1d", "orc_dft1d", "orc_fft3d_r2c", "orc_fft3d_c2r",
                      "orc_bspline_moduli", "orc_scalar_sum", "orc_gather", "orc_eval",
@@ -215,3 +219,63 @@ def evaluate(xyzq, recip3, nfft, order, kappa, nthreads=0):
                                              _p(f), _p(e), _p(es), _p(v), nthreads), "eval")
     return {"force": f, "energy": float(e[0]), "energy_self": float(es[0]),
             "virial": v.reshape(3, 3)}
+
+
+# ---------------------------------------------------------------------------------------------
+# Direct-space nonbonded terms (VDW_VSH + EWALD, the reference's direct test models)
+# ---------------------------------------------------------------------------------------------
+def exclusions_csr(iblo14, inb14, natom, loc2glo=None):
+    """Symmetric 0-based exclusion lists (CSR ptr, idx) from CHARMM's iblo14/inb14 (atom i's
+    partners are |inb14[iblo14[i-1] .. iblo14[i]-1]| - 1, negative entries marking 1-4 pairs;
+    CudaTopExcl.cu:22-80 reads them the same way).  The lists number atoms in their original
+    order; loc2glo[i] (0-based) is the original index of coordinate i, and the result is in the
+    coordinates' order."""
+    iblo14 = np.asarray(iblo14, dtype=np.int64)
+    inb14 = np.asarray(inb14, dtype=np.int64)
+    start = np.r_[0, iblo14[:-1]]
+    ii = np.repeat(np.arange(natom), iblo14 - start)
+    jj = np.abs(inb14) - 1
+    if loc2glo is not None:
+        glo2loc = np.empty(natom, dtype=np.int64)
+        glo2loc[np.asarray(loc2glo, dtype=np.int64)] = np.arange(natom)
+        ii, jj = glo2loc[ii], glo2loc[jj]
+    a = np.r_[ii, jj]
+    b = np.r_[jj, ii]
+    order = np.lexsort((b, a))
+    a, b = a[order], b[order]
+    keep = np.r_[True, (a[1:] != a[:-1]) | (b[1:] != b[:-1])]
+    a, b = a[keep], b[keep]
+    ptr = np.zeros(natom + 1, dtype=np.int32)
+    np.add.at(ptr, a + 1, 1)
+    return np.cumsum(ptr).astype(np.int32), b.astype(np.int32)
+
+
+def direct_force(xyzq, box3, kappa, roff, vdwparam, vdwtype, excl_ptr, excl_idx, nthreads=0):
+    """Main-list pair forces (gradient, (N, 3)), E_vdw, E_elec and the virial (3x3)."""
+    x = np.ascontiguousarray(xyzq, dtype=np.float64).reshape(-1, 4)
+    b = np.ascontiguousarray(box3, dtype=np.float64)
+    vp = np.ascontiguousarray(vdwparam, dtype=np.float64)
+    vt = np.ascontiguousarray(vdwtype, dtype=np.int32)
+    ep = np.ascontiguousarray(excl_ptr, dtype=np.int32)
+    ei = np.ascontiguousarray(excl_idx, dtype=np.int32)
+    f = np.zeros((x.shape[0], 3))
+    ev, ee, v = np.zeros(1), np.zeros(1), np.zeros(9)
+    _check(lib().orc_direct_force(_p(x), x.shape[0], _p(b), float(kappa), float(roff), _p(vp), _p(vt),
+                                  _p(ep), _p(ei), _p(f), _p(ev), _p(ee), _p(v), nthreads), "direct_force")
+    return f, float(ev[0]), float(ee[0]), v.reshape(3, 3)
+
+
+def direct_14(xyzq, box3, kappa, roff, e14fac, vdwparam14, vdwtype, in14, ex14):
+    """1-4 inclusion and exclusion terms: forces (N, 3), E_vdw, E_elec, E_excl, virial."""
+    x = np.ascontiguousarray(xyzq, dtype=np.float64).reshape(-1, 4)
+    b = np.ascontiguousarray(box3, dtype=np.float64)
+    vp = np.ascontiguousarray(vdwparam14, dtype=np.float64)
+    vt = np.ascontiguousarray(vdwtype, dtype=np.int32)
+    i14 = np.ascontiguousarray(in14, dtype=np.int32).reshape(-1, 3)
+    e14 = np.ascontiguousarray(ex14, dtype=np.int32).reshape(-1, 3)
+    f = np.zeros((x.shape[0], 3))
+    ev, ee, ex, v = np.zeros(1), np.zeros(1), np.zeros(1), np.zeros(9)
+    _check(lib().orc_direct_14(_p(x), _p(b), float(kappa), float(roff), float(e14fac), _p(vp), _p(vt),
+                               _p(i14), i14.shape[0], _p(e14), e14.shape[0], _p(f), _p(ev), _p(ee), _p(ex),
+                               _p(v)), "direct_14")
+    return f, float(ev[0]), float(ee[0]), float(ex[0]), v.reshape(3, 3)

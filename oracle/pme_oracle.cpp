@@ -34,6 +34,7 @@
 #include <complex>
 #include <thread>
 #include <algorithm>
+#include <atomic>
 
 typedef std::complex<double> cplx;
 
@@ -713,6 +714,177 @@ extern "C" int orc_eval_tric(const double* xyzq, int natom, const double* recip9
   if (e_recip) *e_recip = e;
   if (vir9) for (int i = 0; i < 9; i++) vir9[i] = v[i];
   if (e_self) *e_self = orc_self_energy(xyzq, natom, kappa);
+  return 0;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Direct-space nonbonded terms (CudaPMEDirectForce, CudaDirectForceKernels.cu), FP64, for the
+// models the reference's test runs: VDW_VSH (shifted Lennard-Jones, :175-195) and EWALD real-space
+// electrostatics (:353-391).  Per pair, with r the minimum-image distance:
+//   U_vdw  = c12/12 (r^-12 + 2 r^6 roff^-18 - 3 roff^-12) - c6/6 (r^-6 + r^6 roff^-12 - 2 roff^-6)
+//   r dU_vdw/dr as the reference writes it: c6 (r^-6 - r^6 roff^-12) - c12 (r^-12 + r^6 roff^-18)
+//     (the sign of its roff^-18 term differs from the derivative of U_vdw; kept, it changes forces
+//     by ~1e-6 kcal/mol/A at roff = 9 A)
+//   U_elec = qq (erfc(kappa r) + s - 1) / r,  r dU_elec/dr = -qq 2/sqrt(pi) kappa exp(-kappa^2 r^2)
+//     - U_elec, qq = ccelec q_i q_j, s = 1 for ordinary pairs, e14fac for 1-4 pairs, 0 for excluded
+//     pairs (the Ewald exclusion correction -qq erf(kappa r)/r)
+//   gradient on i: (r dU/dr) / r^2 * (x_i - x_j); virial_ab -= (r dU/dr) / r^2 dx_a dx_b (the sign
+//     of the reference's virial tensor, gpu_direct.cu:67-70, as for the reciprocal virial).
+// c6/c12 of types (a, b): 6 vdwparam[2 k] and 12 vdwparam[2 k + 1], k = A (A + 1) / 2 + B,
+// A = max, B = min (CudaDirectForce_util.h:265-278; the factors 6 and 12 are applied to the
+// caller's table when it is set, CudaPMEDirectForce.cu:381-387).
+// ---------------------------------------------------------------------------------------------
+struct DirectPair {
+  double f_over_r2, u_vdw, u_elec;
+};
+
+static DirectPair direct_pair(double r2, double qq, double c6, double c12, double kappa, double roff,
+                              double s_elec, bool vdw) {
+  const double r = std::sqrt(r2), rinv = 1.0 / r, rinv2 = rinv * rinv;
+  DirectPair p{0.0, 0.0, 0.0};
+  double fr = 0.0;
+  if (vdw) {
+    const double r6 = r2 * r2 * r2, rinv6 = rinv2 * rinv2 * rinv2, rinv12 = rinv6 * rinv6;
+    const double ro6 = std::pow(roff, -6.0), ro12 = ro6 * ro6, ro18 = ro12 * ro6;
+    p.u_vdw = c12 / 12.0 * (rinv12 + 2.0 * r6 * ro18 - 3.0 * ro12) - c6 / 6.0 * (rinv6 + r6 * ro12 - 2.0 * ro6);
+    fr += c6 * (rinv6 - r6 * ro12) - c12 * (rinv12 + r6 * ro18);
+  }
+  const double e = qq * (std::erfc(kappa * r) + s_elec - 1.0) * rinv;
+  p.u_elec = e;
+  fr += -qq * 2.0 / std::sqrt(kPi) * kappa * std::exp(-kappa * kappa * r2) - e;
+  p.f_over_r2 = fr * rinv2;
+  return p;
+}
+
+static inline void vdw_c6c12(const double* vdwparam, const int* vdwtype, int i, int j, double* c6, double* c12) {
+  const int a = std::max(vdwtype[i], vdwtype[j]), b = std::min(vdwtype[i], vdwtype[j]);
+  const long k = (long)a * (a + 1) / 2 + b;
+  *c6 = 6.0 * vdwparam[2 * k];
+  *c12 = 12.0 * vdwparam[2 * k + 1];
+}
+
+// All pairs within roff (minimum image in the orthorhombic box box3; roff <= min(box)/2), less the
+// excluded pairs excl_idx[excl_ptr[i] .. excl_ptr[i+1]) (0-based, symmetric).  force: AoS
+// (3*natom), overwritten with the gradient; energies and the virial of the pair sum.
+extern "C" int orc_direct_force(const double* xyzq, int natom, const double* box3, double kappa, double roff,
+                                const double* vdwparam, const int* vdwtype, const int* excl_ptr,
+                                const int* excl_idx, double* force, double* e_vdw, double* e_elec,
+                                double* vir9, int nthreads) {
+  if (natom < 0 || !(roff > 0.0) || 2.0 * roff > std::min(box3[0], std::min(box3[1], box3[2]))) return -1;
+  int nc[3];
+  for (int d = 0; d < 3; d++) nc[d] = std::max(1, (int)std::floor(box3[d] / roff));
+  const int ncell = nc[0] * nc[1] * nc[2];
+  std::vector<int> head(ncell, -1), next(natom, -1), cell(natom);
+  auto wrap = [](double x, double L) { return x - L * std::floor(x / L); };
+  for (int i = natom - 1; i >= 0; i--) {
+    int c3[3];
+    for (int d = 0; d < 3; d++) {
+      c3[d] = (int)(wrap(xyzq[4 * i + d], box3[d]) / box3[d] * nc[d]);
+      c3[d] = std::min(std::max(c3[d], 0), nc[d] - 1);
+    }
+    cell[i] = (c3[2] * nc[1] + c3[1]) * nc[0] + c3[0];
+    next[i] = head[cell[i]];
+    head[cell[i]] = i;
+  }
+  const double roff2 = roff * roff;
+  const int T = hw_threads(nthreads);
+  std::vector<double> part((size_t)T * 11, 0.0);
+  std::atomic<int> nexti(0);
+  std::vector<std::thread> th;
+  for (int t = 0; t < T; t++) th.emplace_back([&, t]() {
+    double* acc = &part[(size_t)t * 11];
+    std::vector<char> mark(natom, 0);
+    for (int i = nexti++; i < natom; i = nexti++) {
+      for (int k = excl_ptr[i]; k < excl_ptr[i + 1]; k++) mark[excl_idx[k]] = 1;
+      const int ci = cell[i];
+      const int c3[3] = {ci % nc[0], (ci / nc[0]) % nc[1], ci / (nc[0] * nc[1])};
+      int lo[3], cnt[3];
+      for (int d = 0; d < 3; d++) {
+        if (nc[d] >= 3) { lo[d] = -1; cnt[d] = 3; } else { lo[d] = 0; cnt[d] = nc[d]; }
+      }
+      double fx = 0, fy = 0, fz = 0;
+      for (int oz = 0; oz < cnt[2]; oz++)
+        for (int oy = 0; oy < cnt[1]; oy++)
+          for (int ox = 0; ox < cnt[0]; ox++) {
+            const int z = nc[2] >= 3 ? (c3[2] + lo[2] + oz + nc[2]) % nc[2] : oz;
+            const int y = nc[1] >= 3 ? (c3[1] + lo[1] + oy + nc[1]) % nc[1] : oy;
+            const int x = nc[0] >= 3 ? (c3[0] + lo[0] + ox + nc[0]) % nc[0] : ox;
+            for (int j = head[(z * nc[1] + y) * nc[0] + x]; j >= 0; j = next[j]) {
+              if (j == i || mark[j]) continue;
+              double dx[3];
+              for (int d = 0; d < 3; d++) {
+                dx[d] = xyzq[4 * i + d] - xyzq[4 * j + d];
+                dx[d] -= box3[d] * std::nearbyint(dx[d] / box3[d]);
+              }
+              const double r2 = dx[0] * dx[0] + dx[1] * dx[1] + dx[2] * dx[2];
+              if (!(r2 < roff2)) continue;
+              double c6, c12;
+              vdw_c6c12(vdwparam, vdwtype, i, j, &c6, &c12);
+              const DirectPair p = direct_pair(r2, kCcelec * xyzq[4 * i + 3] * xyzq[4 * j + 3], c6, c12, kappa,
+                                               roff, 1.0, true);
+              fx += p.f_over_r2 * dx[0];
+              fy += p.f_over_r2 * dx[1];
+              fz += p.f_over_r2 * dx[2];
+              acc[0] += 0.5 * p.u_vdw;
+              acc[1] += 0.5 * p.u_elec;
+              for (int a = 0; a < 3; a++)
+                for (int b = 0; b < 3; b++) acc[2 + 3 * a + b] -= 0.5 * p.f_over_r2 * dx[a] * dx[b];
+            }
+          }
+      force[3 * i + 0] = fx;
+      force[3 * i + 1] = fy;
+      force[3 * i + 2] = fz;
+      for (int k = excl_ptr[i]; k < excl_ptr[i + 1]; k++) mark[excl_idx[k]] = 0;
+    }
+  });
+  for (auto& x : th) x.join();
+  double s[11] = {0};
+  for (int t = 0; t < T; t++)
+    for (int c = 0; c < 11; c++) s[c] += part[(size_t)t * 11 + c];
+  if (e_vdw) *e_vdw = s[0];
+  if (e_elec) *e_elec = s[1];
+  if (vir9) for (int c = 0; c < 9; c++) vir9[c] = s[2 + c];
+  return 0;
+}
+
+// The 1-4 lists (CudaDirectForceKernels.cu:504-640): in14 (i, j, ishift) triples get the 1-4 vdW
+// parameters and electrostatics scaled as erfc + e14fac - 1; ex14 triples the exclusion correction
+// (e14fac 0); no cutoff test, the VSH shift uses roff.  ishift encodes the periodic image of j: shift_d = (digit_d - 1) box_d with
+// ishift = dx + 3 dy + 9 dz digits (gpu_utils.h:312-320).  force (AoS) is ADDED to.
+extern "C" int orc_direct_14(const double* xyzq, const double* box3, double kappa, double roff, double e14fac,
+                             const double* vdwparam14, const int* vdwtype, const int* in14, int nin14,
+                             const int* ex14, int nex14, double* force, double* e_vdw, double* e_elec,
+                             double* e_excl, double* vir9) {
+  double ev = 0, ee = 0, ex = 0, w[9] = {0};
+  for (int pass = 0; pass < 2; pass++) {
+    const int* L = pass == 0 ? in14 : ex14;
+    const int n = pass == 0 ? nin14 : nex14;
+    for (int k = 0; k < n; k++) {
+      const int i = L[3 * k], j = L[3 * k + 1];
+      int ish = L[3 * k + 2];
+      const double sh[3] = {(double)(ish % 3 - 1) * box3[0], (double)((ish / 3) % 3 - 1) * box3[1],
+                            (double)(ish / 9 - 1) * box3[2]};
+      double dx[3];
+      for (int d = 0; d < 3; d++) dx[d] = xyzq[4 * i + d] - xyzq[4 * j + d] + sh[d];
+      const double r2 = dx[0] * dx[0] + dx[1] * dx[1] + dx[2] * dx[2];
+      const double qq = kCcelec * xyzq[4 * i + 3] * xyzq[4 * j + 3];
+      double c6 = 0, c12 = 0;
+      if (pass == 0) vdw_c6c12(vdwparam14, vdwtype, i, j, &c6, &c12);
+      // no cutoff test for listed pairs; the VSH shift terms use roff as for the main pairs
+      const DirectPair p = direct_pair(r2, qq, c6, c12, kappa, roff, pass == 0 ? e14fac : 0.0, pass == 0);
+      for (int d = 0; d < 3; d++) {
+        force[3 * i + d] += p.f_over_r2 * dx[d];
+        force[3 * j + d] -= p.f_over_r2 * dx[d];
+      }
+      if (pass == 0) { ev += p.u_vdw; ee += p.u_elec; } else { ex += p.u_elec; }
+      for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++) w[3 * a + b] -= p.f_over_r2 * dx[a] * dx[b];
+    }
+  }
+  if (e_vdw) *e_vdw = ev;
+  if (e_elec) *e_elec = ee;
+  if (e_excl) *e_excl = ex;
+  if (vir9) for (int c = 0; c < 9; c++) vir9[c] = w[c];
   return 0;
 }
 

@@ -16,6 +16,17 @@ It writes, next to this script:
   (test_data/dataFFT{in,out}{64,64x2,64x64,4x4}.txt, used by test_fbfft.cu:188-256): real
   inputs (rows, x fastest) and their full complex DFTs (sign -1, unnormalised).
 
+* ``ref_direct_23558.npz`` -- the reference direct-space test (gpu_direct.cu:55-207): the same
+  23,558 atoms with their vdW types (test_data/vdwtype.txt) and parameters
+  (test_data/vdwparam.txt, vdwparam14.txt: (c6, c12) pairs of 35 types), the CHARMM exclusion
+  lists (iblo14.txt, inb14.txt, in the original atom order), the map from the coordinates'
+  order to that order (loc2glo.txt, stored 0-based; xyzq.txt is the reference's neighbour-list
+  order), the 1-4 inclusion and exclusion lists (in14list.txt,
+  ex14list.txt), the settings of gpu_direct.cu:58-66 (box 62.23 A, kappa 0.32, roff 9, ron 7.5,
+  e14fac 1.5, VDW_VSH + EWALD), the expected main-list and total forces (force_direct_main.txt,
+  force_direct.txt), energies, virial and the driver's tolerances (gpu_direct.cu:67-76, 158,
+  171, 203-207, 222).
+
 Nothing at run time reads the reference tree: the tests load these .npz files.
 """
 from __future__ import annotations
@@ -68,6 +79,30 @@ def main(ref_root: str) -> None:
         kat[f"in{tag}"] = xin
         kat[f"out{tag}"] = xout
     np.savez_compressed(os.path.join(HERE, "fft_kat.npz"), **kat)
+
+    def ints(name, cols=1):
+        a = np.loadtxt(os.path.join(td, name), dtype=np.int64)
+        return a.reshape(-1, cols).astype(np.int32) if cols > 1 else a.astype(np.int32)
+
+    direct = dict(
+        xyzq=xyzq, box=np.array([62.23, 62.23, 62.23]), kappa=np.array(0.320), roff=np.array(9.0),
+        ron=np.array(7.5), e14fac=np.array(1.5),
+        vdwparam=np.loadtxt(os.path.join(td, "vdwparam.txt"), dtype=np.float64),
+        vdwparam14=np.loadtxt(os.path.join(td, "vdwparam14.txt"), dtype=np.float64),
+        vdwtype=ints("vdwtype.txt"), iblo14=ints("iblo14.txt"), inb14=ints("inb14.txt"),
+        loc2glo=ints("loc2glo.txt") - 1,
+        in14=ints("in14list.txt", 3), ex14=ints("ex14list.txt", 3),
+        force_main=np.loadtxt(os.path.join(td, "force_direct_main.txt"), dtype=np.float64),
+        force_total=np.loadtxt(os.path.join(td, "force_direct.txt"), dtype=np.float64),
+        energy_vdw=np.array(8198.14425), energy_elec=np.array(-73396.45998),
+        virial=np.array([58748.2766568620, 159.656334638237, 483.080609561938,
+                         159.656334638202, 57272.9410562695, 894.635309171291,
+                         483.080609561938, 894.635309171288, 56639.3675265570]).reshape(3, 3),
+        tol_force_main=np.array(7.72e-4), tol_force_total=np.array(7.73e-4),
+        tol_energy=np.array(0.007), tol_virial=np.array(3.13))
+    assert direct["vdwparam"].shape == (1260,) and direct["in14"].shape == (6556, 3)
+    assert direct["force_main"].shape == (23558, 3) and direct["inb14"].shape == (34709,)
+    np.savez_compressed(os.path.join(HERE, "ref_direct_23558.npz"), **direct)
     print("wrote", sorted(os.listdir(HERE)))
 
 
