@@ -1,4 +1,4 @@
-"""ctypes bindings of the C ABI in include/pme_recip.h (libpme_b200.so).
+"""ctypes bindings of the C ABI in include/pme_recip.h and include/pme_direct.h (libpme_b200.so).
 
 The shared library is built in-tree by gpu_recip_b200/build.py.  There is no fallback: if the
 library is missing or fails to load, every entry point raises.
@@ -22,6 +22,8 @@ PME_ESTATE = -6
 PME_FFT_COLUMN, PME_FFT_SLAB, PME_FFT_BOX = 0, 1, 2
 PME_FORCE_F32_SOA, PME_FORCE_F32X3, PME_FORCE_I64_SOA_ACCUM = 0, 1, 2
 PME_EV_RECIP, PME_EV_SELF, PME_EV_VIRIAL, PME_EV_COUNT = 0, 1, 2, 11
+PME_VDW_NONE, PME_VDW_VSH = 0, 1
+PME_ELEC_NONE, PME_ELEC_EWALD = 0, 101
 
 _P = ctypes.c_void_p
 _I = ctypes.c_int
@@ -83,6 +85,20 @@ SIGNATURES = {
     "pme_server_submit": [_P, _P, ctypes.POINTER(ctypes.c_longlong)],
     "pme_server_wait": [_P, ctypes.c_longlong, _D, _DP],
     "pme_server_get_stats": [_P, _P],
+    "pme_direct_create": [_P, ctypes.POINTER(_P)],
+    "pme_direct_destroy": [_P],
+    "pme_direct_set_stream": [_P, _P],
+    "pme_direct_setup": [_P, _D, _D, _D, _D, _D, _D, _D, _I, _I],
+    "pme_direct_set_box_size": [_P, _D, _D, _D],
+    "pme_direct_set_vdwparam": [_P, _I, _P],
+    "pme_direct_set_vdwparam14": [_P, _I, _P],
+    "pme_direct_set_vdwtype": [_P, _I, _P],
+    "pme_direct_set_exclusions": [_P, _I, _P, _P, _P],
+    "pme_direct_set_14_list": [_P, _I, _I, _P, _P],
+    "pme_direct_calc_force": [_P, _P, _I, _I, _I, _I, _P],
+    "pme_direct_calc_14_force": [_P, _P, _I, _I, _I, _P],
+    "pme_direct_clear_energy_virial": [_P],
+    "pme_direct_get_energy_virial": [_P, _DP, _DP, _DP, _DP],
     "pme_last_error_string": [],
     "pme_status_string": [_I],
     "pme_version": [],
