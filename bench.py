@@ -55,6 +55,8 @@ def parse():
     ap.add_argument("--large-steps", type=int, default=20, help="timed evaluations of the 216^3 system (0: skip)")
     ap.add_argument("--triclinic-steps", type=int, default=200,
                     help="timed evaluations of the 24,000-atom rhombic dodecahedron (0: skip)")
+    ap.add_argument("--direct-steps", type=int, default=200,
+                    help="timed direct-space evaluations of the reference's 23,558-atom system (0: skip)")
     ap.add_argument("--serve-requests", type=int, default=600, help="requests of the serving run (0: skip)")
     ap.add_argument("--serve-rate", type=float, default=400.0, help="Poisson arrival rate (requests/s)")
     return ap.parse_args()
@@ -319,6 +321,11 @@ def run_b200(args):
     if args.triclinic_steps > 0:
         triclinic = run_triclinic(args, dev, stream, flush, rank, world)
 
+    # ---- direct space: the reference's direct-test system, and a whole Ewald step ------------------
+    direct = None
+    if args.direct_steps > 0:
+        direct = run_direct(args, dev, stream, flush, rank, world)
+
     # ---- serving: Poisson request stream, continuous batching vs the plain path ------------------
     serving = None
     if args.serve_requests > 0:
@@ -343,7 +350,7 @@ def run_b200(args):
                         "d2h_bytes_per_step": 4 * 3 * stride + 8 * 11},
                 "gpu_launches": kernels_per_eval * K,
                 "roofline": roofline, "batched": batched, "serving": serving, "large": large,
-                "triclinic": triclinic,
+                "triclinic": triclinic, "direct": direct,
                 "fft_comparator": fft_cmp,
                 "clocks": clocks.summary(), "cpu_baseline": cpu}
         print(json.dumps(line), flush=True)
@@ -499,6 +506,84 @@ def run_triclinic(args, dev, stream, flush, rank, world):
             "steps": K, "ms_per_eval": ms, "evals_per_s": R.aggregate_rate([K] * world, total / 1000.0),
             "alg_bytes_per_eval": s.alg_bytes(),
             "roofline_frac": s.alg_bytes() / (ms * 1e-3) / 1e9 / peak}
+
+
+def run_direct(args, dev, stream, flush, rank, world):
+    """Direct-space PME on the reference's direct test system (tests/golden/ref_direct_23558.npz:
+    23,558 atoms, 62.23 A box, roff 9 A, kappa 0.32, 35 vdW types, CHARMM exclusions, 6,556 1-4
+    and 28,153 excluded pairs): the main pair list, main + 1-4 lists, and a whole Ewald step
+    (direct + 1-4 + reciprocal 64^3 order 4) on the same coordinates, L2 flushed between steps.
+    The FP64 oracle's main list on all host threads beside it."""
+    import torch
+    from gpu_recip_b200 import CudaPMERecip, force_stride
+    from gpu_recip_b200 import replicas as R
+    from gpu_recip_b200.direct import CudaPMEDirectForce
+    d = dict(np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "tests", "golden",
+                                  "ref_direct_23558.npz")))
+    n = d["xyzq"].shape[0]
+    dr = CudaPMEDirectForce(stream=stream)
+    dr.setup(*d["box"], float(d["kappa"]), float(d["roff"]), float(d["ron"]), float(d["e14fac"]))
+    dr.set_vdwparam(d["vdwparam"])
+    dr.set_vdwparam14(d["vdwparam14"])
+    dr.set_vdwtype(d["vdwtype"])
+    dr.set_exclusions(d["iblo14"], d["inb14"], d["loc2glo"])
+    dr.set_14_list(d["in14"], d["ex14"])
+    x = torch.from_numpy(np.ascontiguousarray(d["xyzq"], dtype=np.float32)).to(dev)
+    stride = force_stride(n, 8)
+    fi = torch.zeros(3 * stride, dtype=torch.int64, device=dev)
+    pme = CudaPMERecip(64, 64, 64, 4, stream=stream)
+    inv = [1.0 / float(b) for b in d["box"]]
+    K = args.direct_steps
+    W = max(3, args.warmup)
+
+    def timed(body):
+        e0 = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+        e1 = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+        with torch.cuda.stream(stream):
+            for i in range(K + W):
+                flush.fill_(float(i & 7))
+                if i >= W:
+                    e0[i - W].record(stream)
+                body()
+                if i >= W:
+                    e1[i - W].record(stream)
+        stream.synchronize()
+        return R.max_over_ranks(float(sum(e0[i].elapsed_time(e1[i]) for i in range(K))), dev) / K
+
+    def main_only():
+        dr.energy_virial.clear()
+        dr.calc_force(x, n, True, True, stride, fi)
+
+    def with14():
+        main_only()
+        dr.calc_14_force(x, True, True, stride, fi)
+
+    def ewald():
+        with14()
+        pme.energy_virial.clear()
+        pme.eval_ortho(inv, x, n, float(d["kappa"]), True, True, fi, stride)
+
+    ms_main = timed(main_only)
+    ms_14 = timed(with14)
+    ms_ewald = timed(ewald)
+    dr.close()
+    pme.close()
+    out = {"workload": "ref_direct_23558: the reference's direct-space test system, 23,558 atoms, box 62.23 A, "
+                       "roff 9 A, kappa 0.32, VDW_VSH + EWALD, 35 vdW types, CHARMM exclusions, 1-4 lists",
+           "steps": K, "ms_main_list": ms_main, "ms_with_14_lists": ms_14,
+           "direct_evals_per_s": R.aggregate_rate([K] * world, ms_14 * K / 1000.0),
+           "ewald_step_ms": ms_ewald, "ewald_steps_per_s": R.aggregate_rate([K] * world, ms_ewald * K / 1000.0),
+           "ewald_step": "direct main + 1-4 lists + reciprocal (64^3, order 4), one int64 force array",
+           "launches_per_direct_eval": 6}
+    if rank == 0 and not args.no_cpu_baseline:
+        from oracle import oracle as O
+        ptr, idx = O.exclusions_csr(d["iblo14"], d["inb14"], n, d["loc2glo"])
+        t0 = time.perf_counter()
+        O.direct_force(d["xyzq"].astype(np.float64), d["box"], float(d["kappa"]), float(d["roff"]), d["vdwparam"],
+                       d["vdwtype"], ptr, idx)
+        out["cpu_oracle_ms_main_list"] = (time.perf_counter() - t0) * 1000.0
+        out["cpu_oracle_cores"] = O.hardware_threads()
+    return out
 
 
 def serving_stream(n: int, rate: float, seed: int):

@@ -10,12 +10,14 @@
 //   k_direct_fill   atoms into their cells (unordered);
 //   k_direct_order  one warp per cell: order the cell's atoms by index (so every run sums in the
 //                   same order) and gather coordinates, type, global index and exclusion window;
-//   k_direct_pairs  one warp per 32 atoms of a cell (lane = atom i) against every atom of the
-//                   3 x 5 x 5 neighbouring cells, staged 32 at a time in shared memory.
-// Each pair is evaluated from both sides (no third-law scatter): an atom's force is a register
-// sum in a fixed order, added once to the int64 output at 2^40, so results are run-to-run
-// identical.  Energies are rounded to 2^-32 per pair and summed in int64 (exact); both sides of a
-// pair give the same bits, so the doubled sums halve exactly (1-4 terms are added twice to match).
+//   k_direct_pairs  one warp per 32 atoms of a cell (lane = atom i) and z slice of its 3 x 5 x 5
+//                   neighbouring cells: a cheap distance/exclusion pass compacts the pairs within
+//                   roff, whose terms then run on full lanes.
+// Each pair is evaluated from both sides (no third-law scatter): each pair's force is rounded once
+// to 2^-40 and every sum after that is exact int64, so results are run-to-run identical and the
+// only FP32 error is that of the pair terms themselves.  Energies are rounded to 2^-32 per pair and summed in int64; both sides
+// give the same pair distance (dx = (x_i - x_j) - shift is antisymmetric), so the doubled sums
+// halve exactly (1-4 terms are added twice to match).
 // Exclusions: a 128-bit window per atom over global indices g_j - g_i in [-64, 64) (bit 64: the
 // atom itself), plus an explicit list for partners beyond the window.
 #include <cuda_runtime.h>
@@ -32,7 +34,6 @@ namespace pme {
 namespace direct {
 
 constexpr int kWarps = 8;             // warps per CTA of the pair kernel (256 threads)
-constexpr int kChunkStride = 4;       // warps per cell: a cell's 32-atom chunks k, k+4, k+8, ...
 constexpr int kMaxTypes = 200;        // vdW types (packed pairs held in shared memory)
 constexpr float kEnergyScale = 4294967296.0f;     // 2^32
 constexpr float kForceScaleF = 1099511627776.0f;  // 2^40
@@ -46,6 +47,8 @@ struct Params {
   int nc[3];          // cells per axis
   int lo[3], cnt[3];  // neighbour cell offsets per axis: lo .. lo + cnt - 1
   int npair;          // vdW type pairs
+  double kappad, ro6d, ro12d, ro18d;   // FP64 copies for the main-list pair terms
+  double boxd[3];
 };
 
 enum Acc { kAccVdw = 0, kAccElec = 1, kAccExcl = 2, kAccVir = 3, kAccN = 9 };   // vir: xx xy xz yy yz zz
@@ -56,8 +59,8 @@ enum Acc { kAccVdw = 0, kAccElec = 1, kAccExcl = 2, kAccVir = 3, kAccN = 9 };   
 // c6 / c12 carry the reference's factors 6 and 12.
 __device__ __forceinline__ float pair_terms(float r2, float qq, float c6, float c12, const Params& p, int kind,
                                             bool vdw, float& u_vdw, float& u_elec) {
-  const float rinv = rsqrtf(r2);
-  const float r = r2 * rinv;
+  const float r = sqrtf(r2);        // IEEE square root and reciprocal, as the reference computes them
+  const float rinv = 1.0f / r;
   const float rinv2 = rinv * rinv;
   float fr = 0.0f;
   u_vdw = 0.0f;
@@ -75,6 +78,28 @@ __device__ __forceinline__ float pair_terms(float r2, float qq, float c6, float 
   return fr * rinv2;
 }
 
+// The same terms in FP64 from the FP32 pair geometry, for the main pair list: the atoms' net
+// forces are small differences of large pair forces (close contacts of ~1e3 kcal/mol/A), where
+// the few-ulp error of an FP32 evaluation shows.
+__device__ __forceinline__ double pair_terms_f64(double r2, double qq, double c6, double c12, const Params& p,
+                                                 bool vdw, double& u_vdw, double& u_elec) {
+  const double rinv = rsqrt(r2);
+  const double r = r2 * rinv;
+  const double rinv2 = rinv * rinv;
+  double fr = 0.0;
+  u_vdw = 0.0;
+  if (vdw) {
+    const double rinv6 = rinv2 * rinv2 * rinv2, rinv12 = rinv6 * rinv6, r6 = r2 * r2 * r2;
+    fr = c6 * (rinv6 - r6 * p.ro12d) - c12 * (rinv12 + r6 * p.ro18d);
+    u_vdw = c12 * (1.0 / 12.0) * (rinv12 + 2.0 * r6 * p.ro18d - 3.0 * p.ro12d) -
+            c6 * (1.0 / 6.0) * (rinv6 + r6 * p.ro12d - 2.0 * p.ro6d);
+  }
+  const double e = qq * erfc(p.kappad * r) * rinv;
+  u_elec = e;
+  fr += -qq * 1.1283791670955126 * p.kappad * exp(-p.kappad * p.kappad * r2) - e;
+  return fr * rinv2;
+}
+
 __device__ __forceinline__ float2 vdw_c6c12(const float2* tab, int ta, int tb) {
   const int a = max(ta, tb), b = min(ta, tb);
   return tab[a * (a + 1) / 2 + b];
@@ -89,11 +114,16 @@ __device__ __forceinline__ long long warp_sum_ll(long long v) {
 // ---------------------------------------------------------------------------------------------
 // Binning
 // ---------------------------------------------------------------------------------------------
-__device__ __forceinline__ int cell_of_coord(float x, float inv_box, int n) {
-  float s = x * inv_box;
-  s -= floorf(s);
-  if (!(s >= 0.0f && s < 1.0f)) s = 0.0f;   // non-finite coordinates go to cell 0
-  return min((int)(s * (float)n), n - 1);
+// Coordinate wrapped into the box: x - L floor(x / L), which FP32 rounding can leave a hair below
+// 0 or equal to L; non-finite inputs become 0.  The cell comes from this same value, so an atom's
+// cell and its stored position always agree (the cells are wider than their reach by a margin).
+__device__ __forceinline__ float wrap_coord(float x, float box, float inv_box) {
+  const float w = x - box * floorf(x * inv_box);
+  return (w >= -box && w <= 2.0f * box) ? w : 0.0f;
+}
+
+__device__ __forceinline__ int cell_of_wrapped(float w, float inv_box, int n) {
+  return max(0, min((int)(w * inv_box * (float)n), n - 1));
 }
 
 __global__ void k_direct_cell(const float4* __restrict__ xyzq, int n, const Params p, int* __restrict__ cell_of,
@@ -101,37 +131,50 @@ __global__ void k_direct_cell(const float4* __restrict__ xyzq, int n, const Para
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const float4 a = xyzq[i];
-  const int cx = cell_of_coord(a.x, p.inv_box[0], p.nc[0]);
-  const int cy = cell_of_coord(a.y, p.inv_box[1], p.nc[1]);
-  const int cz = cell_of_coord(a.z, p.inv_box[2], p.nc[2]);
+  const int cx = cell_of_wrapped(wrap_coord(a.x, p.box[0], p.inv_box[0]), p.inv_box[0], p.nc[0]);
+  const int cy = cell_of_wrapped(wrap_coord(a.y, p.box[1], p.inv_box[1]), p.inv_box[1], p.nc[1]);
+  const int cz = cell_of_wrapped(wrap_coord(a.z, p.box[2], p.inv_box[2]), p.inv_box[2], p.nc[2]);
   const int c = (cz * p.nc[1] + cy) * p.nc[0] + cx;
   cell_of[i] = c;
   atomicAdd(&count[c], 1);
 }
 
-// Exclusive scan of count[0..ncell) into start[0..ncell]; one CTA of 1024 threads, each owning a
+// Exclusive scans of count[0..ncell) into start[0..ncell] (atoms) and of ceil(count / 32) into
+// chunk[0..ncell] (32-atom chunks, chunk[ncell] the total); one CTA of 1024 threads, each owning a
 // contiguous run of cells.
-__global__ void __launch_bounds__(1024) k_direct_scan(const int* __restrict__ count, int ncell, int* __restrict__ start) {
-  __shared__ int part[1024];
+__global__ void __launch_bounds__(1024) k_direct_scan(const int* __restrict__ count, int ncell, int* __restrict__ start,
+                                                      int* __restrict__ chunk) {
+  __shared__ int part[1024], partc[1024];
   const int t = threadIdx.x;
   const int per = (ncell + 1023) / 1024;
   const int b = min(t * per, ncell), e = min(b + per, ncell);
-  int s = 0;
-  for (int c = b; c < e; c++) s += count[c];
+  int s = 0, sc = 0;
+  for (int c = b; c < e; c++) {
+    s += count[c];
+    sc += (count[c] + 31) >> 5;
+  }
   part[t] = s;
+  partc[t] = sc;
   __syncthreads();
-  for (int off = 1; off < 1024; off <<= 1) {   // inclusive Hillis-Steele scan of the run sums
+  for (int off = 1; off < 1024; off <<= 1) {   // inclusive Hillis-Steele scans of the run sums
     const int v = t >= off ? part[t - off] : 0;
+    const int vc = t >= off ? partc[t - off] : 0;
     __syncthreads();
     part[t] += v;
+    partc[t] += vc;
     __syncthreads();
   }
-  int run = part[t] - s;
+  int run = part[t] - s, runc = partc[t] - sc;
   for (int c = b; c < e; c++) {
     start[c] = run;
+    chunk[c] = runc;
     run += count[c];
+    runc += (count[c] + 31) >> 5;
   }
-  if (t == 1023) start[ncell] = part[1023];
+  if (t == 1023) {
+    start[ncell] = part[1023];
+    chunk[ncell] = partc[1023];
+  }
 }
 
 __global__ void k_direct_fill(const int* __restrict__ cell_of, int n, const int* __restrict__ start,
@@ -146,7 +189,8 @@ __global__ void k_direct_fill(const int* __restrict__ cell_of, int n, const int*
 __global__ void k_direct_order(const int* __restrict__ start, int ncell, const int* __restrict__ tmp,
                                const float4* __restrict__ xyzq, const int* __restrict__ vdwtype,
                                const int* __restrict__ glob, const ulonglong2* __restrict__ win,
-                               const int* __restrict__ far_ptr, float4* __restrict__ pos, int4* __restrict__ info,
+                               const int* __restrict__ far_ptr, float box_x, float box_y, float box_z, float inv_x,
+                               float inv_y, float inv_z, float4* __restrict__ pos, int4* __restrict__ info,
                                ulonglong2* __restrict__ mask) {
   const int lane = threadIdx.x & 31;
   for (int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < ncell; c += (gridDim.x * blockDim.x) >> 5) {
@@ -156,7 +200,11 @@ __global__ void k_direct_order(const int* __restrict__ start, int ncell, const i
       int rank = 0;
       for (int m = s; m < e; m++) rank += tmp[m] < a ? 1 : 0;
       const int d = s + rank;
-      pos[d] = xyzq[a];
+      float4 q = xyzq[a];   // wrapped: neighbour cells then need only their periodic shift
+      q.x = wrap_coord(q.x, box_x, inv_x);
+      q.y = wrap_coord(q.y, box_y, inv_y);
+      q.z = wrap_coord(q.z, box_z, inv_z);
+      pos[d] = q;
       info[d] = make_int4(vdwtype[a], glob[a], a, far_ptr[a + 1] > far_ptr[a] ? 1 : 0);
       mask[d] = win[a];
     }
@@ -173,83 +221,192 @@ __device__ __forceinline__ bool far_excluded(const int* __restrict__ far_ptr, co
   return false;
 }
 
-__global__ void __launch_bounds__(kWarps * 32) k_direct_pairs(
-    const Params p, const int* __restrict__ start, const float4* __restrict__ pos, const int4* __restrict__ info,
+// One warp per (cell, 32-atom chunk of it, z slice of its neighbour cells): lane = atom i.  For
+// each batch of 32 j atoms staged in shared memory, a cheap pass tests the 32 x 32 pairs (distance
+// with the neighbour cell's periodic shift, or the minimum image when an axis has too few cells,
+// then the exclusion window) and compacts the hits into a per-warp list; the pair terms then run
+// in FP64 (from the FP32 positions, exactly) on full lanes, 32 hits at a time (the list is ordered
+// by i, so a segmented warp scan folds each i's run into one add to its shared-memory
+// accumulator).  Every pair force is rounded once to 2^-40 and summed in
+// int64 from there on (exact: no accumulation error, and no dependence on the order of the adds
+// or of the slices).  FP64 because an atom's net force is a small difference of large pair forces,
+// where the few-ulp error of FP32 pair terms reaches ~1e-5 kcal/mol/A.
+template <bool MINIMG>
+__global__ void __launch_bounds__(kWarps * 32, 3) k_direct_pairs(
+    const Params p, const int* __restrict__ start, const int* __restrict__ chunkp, const float4* __restrict__ pos,
+    const int4* __restrict__ info,
     const ulonglong2* __restrict__ mask, const int* __restrict__ far_ptr, const int* __restrict__ far_idx,
     const float2* __restrict__ vdwp, int calc_energy, int calc_virial, int stride, long long* __restrict__ force,
     long long* __restrict__ acc) {
   extern __shared__ float2 sh_vdw[];
-  __shared__ float4 sh_pos[kWarps][32];
-  __shared__ int2 sh_tg[kWarps][32];
+  __shared__ float4 sh_jpos[kWarps][32];
+  __shared__ int2 sh_jtg[kWarps][32];
+  __shared__ float4 sh_ipos[kWarps][32];
+  __shared__ int sh_itype[kWarps][32];
+  __shared__ long long sh_f[kWarps][3][32];   // force sums at 2^40 (exact)
+  __shared__ unsigned short sh_items[kWarps][1024];
   for (int k = threadIdx.x; k < p.npair; k += blockDim.x) sh_vdw[k] = vdwp[k];
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int ncell = p.nc[0] * p.nc[1] * p.nc[2];
+  const int nslice = p.cnt[2];
   const bool vdw_on = p.vdw != PME_VDW_NONE;
-  for (int task = blockIdx.x * kWarps + warp; task < ncell * kChunkStride; task += gridDim.x * kWarps) {
-    const int c = task / kChunkStride;
-    const int cs = start[c], ce = start[c + 1];
+  long long ev = 0, ee = 0;
+  double w0 = 0.0, w1 = 0.0, w2 = 0.0, w3 = 0.0, w4 = 0.0, w5 = 0.0;
+  const int nchunk = chunkp[ncell];
+  const int ntask = nchunk * nslice;
+  for (int task = blockIdx.x * kWarps + warp; task < ntask; task += gridDim.x * kWarps) {
+    const int sl = task % nslice;
+    const int g = task / nslice;
+    int clo = 0, chi = ncell - 1;   // the cell holding chunk g: last c with chunkp[c] <= g
+    while (clo < chi) {
+      const int mid = (clo + chi + 1) >> 1;
+      if (chunkp[mid] <= g) clo = mid; else chi = mid - 1;
+    }
+    const int c = clo;
+    const int ce = start[c + 1];
     const int cx = c % p.nc[0], cy = (c / p.nc[0]) % p.nc[1], cz = c / (p.nc[0] * p.nc[1]);
-    for (int chunk = cs + (task % kChunkStride) * 32; chunk < ce; chunk += kChunkStride * 32) {
+    {
+      const int chunk = start[c] + (g - chunkp[c]) * 32;
       const int i = chunk + lane;
       const bool act = i < ce;
       const float4 pi = act ? pos[i] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
       const int4 ii = act ? info[i] : make_int4(0, 0, 0, 0);
       const ulonglong2 mi = act ? mask[i] : make_ulonglong2(0ull, 0ull);
-      float fx = 0.0f, fy = 0.0f, fz = 0.0f;
-      float w0 = 0.0f, w1 = 0.0f, w2 = 0.0f, w3 = 0.0f, w4 = 0.0f, w5 = 0.0f;
-      long long ev = 0, ee = 0;
-      for (int oz = 0; oz < p.cnt[2]; oz++) {
-        const int z = p.cnt[2] == p.nc[2] ? oz : (cz + p.lo[2] + oz + p.nc[2]) % p.nc[2];
-        for (int oy = 0; oy < p.cnt[1]; oy++) {
-          const int y = p.cnt[1] == p.nc[1] ? oy : (cy + p.lo[1] + oy + p.nc[1]) % p.nc[1];
-          for (int ox = 0; ox < p.cnt[0]; ox++) {
-            const int x = p.cnt[0] == p.nc[0] ? ox : (cx + p.lo[0] + ox + p.nc[0]) % p.nc[0];
-            const int cn = (z * p.nc[1] + y) * p.nc[0] + x;
-            const int js = start[cn], je = start[cn + 1];
-            for (int b = js; b < je; b += 32) {
-              if (b + lane < je) {
-                sh_pos[warp][lane] = pos[b + lane];
-                const int4 jt = info[b + lane];
-                sh_tg[warp][lane] = make_int2(jt.x, jt.y);
-              }
-              __syncwarp();
-              const int nb = min(32, je - b);
-              if (act) {
-                for (int t = 0; t < nb; t++) {
-                  const float4 pj = sh_pos[warp][t];
-                  float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+      sh_ipos[warp][lane] = pi;
+      sh_itype[warp][lane] = ii.x;
+      sh_f[warp][0][lane] = 0;
+      sh_f[warp][1][lane] = 0;
+      sh_f[warp][2][lane] = 0;
+      // this task's z slice of the neighbour cells, with its periodic shift
+      int z = MINIMG && p.cnt[2] == p.nc[2] ? sl : cz + p.lo[2] + sl;
+      float shz = 0.0f;
+      if (!MINIMG) {
+        if (z < 0) { z += p.nc[2]; shz = -p.box[2]; } else if (z >= p.nc[2]) { z -= p.nc[2]; shz = p.box[2]; }
+      } else if (p.cnt[2] != p.nc[2]) {
+        z = (z + p.nc[2]) % p.nc[2];
+      }
+      __syncwarp();
+      for (int oy = 0; oy < p.cnt[1]; oy++) {
+        int y = MINIMG && p.cnt[1] == p.nc[1] ? oy : cy + p.lo[1] + oy;
+        float shy = 0.0f;
+        if (!MINIMG) {
+          if (y < 0) { y += p.nc[1]; shy = -p.box[1]; } else if (y >= p.nc[1]) { y -= p.nc[1]; shy = p.box[1]; }
+        } else if (p.cnt[1] != p.nc[1]) {
+          y = (y + p.nc[1]) % p.nc[1];
+        }
+        for (int ox = 0; ox < p.cnt[0]; ox++) {
+          int x = MINIMG && p.cnt[0] == p.nc[0] ? ox : cx + p.lo[0] + ox;
+          float shx = 0.0f;
+          if (!MINIMG) {
+            if (x < 0) { x += p.nc[0]; shx = -p.box[0]; } else if (x >= p.nc[0]) { x -= p.nc[0]; shx = p.box[0]; }
+          } else if (p.cnt[0] != p.nc[0]) {
+            x = (x + p.nc[0]) % p.nc[0];
+          }
+          const int cn = (z * p.nc[1] + y) * p.nc[0] + x;
+          const int js = start[cn], je = start[cn + 1];
+          for (int b = js; b < je; b += 32) {
+            if (b + lane < je) {
+              sh_jpos[warp][lane] = pos[b + lane];
+              const int4 jt = info[b + lane];
+              sh_jtg[warp][lane] = make_int2(jt.x, jt.y);
+            }
+            __syncwarp();
+            const int nb = min(32, je - b);
+            // cheap pass: which of the batch's j are partners of this lane's i
+            unsigned hits = 0u;
+            if (act) {
+              for (int t = 0; t < nb; t++) {
+                const float4 pj = sh_jpos[warp][t];
+                float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+                if (MINIMG) {
                   dx -= p.box[0] * rintf(dx * p.inv_box[0]);
                   dy -= p.box[1] * rintf(dy * p.inv_box[1]);
                   dz -= p.box[2] * rintf(dz * p.inv_box[2]);
-                  const float r2 = dx * dx + dy * dy + dz * dz;
-                  if (!(r2 < p.roff2)) continue;
-                  const int2 tg = sh_tg[warp][t];
-                  const unsigned k = (unsigned)(tg.y - ii.y + 64);
+                } else {
+                  dx -= shx; dy -= shy; dz -= shz;
+                }
+                const float r2 = dx * dx + dy * dy + dz * dz;
+                if (r2 < p.roff2) {
+                  const unsigned k = (unsigned)(sh_jtg[warp][t].y - ii.y + 64);
                   bool excl;
                   if (k < 128u) {
-                    const unsigned long long wbits = k < 64u ? mi.x : mi.y;
-                    excl = ((wbits >> (k & 63u)) & 1ull) != 0ull;
+                    const unsigned long long wb = k < 64u ? mi.x : mi.y;
+                    excl = ((wb >> (k & 63u)) & 1ull) != 0ull;
                   } else {
-                    excl = ii.w != 0 && far_excluded(far_ptr, far_idx, ii.z, tg.y);
+                    excl = ii.w != 0 && far_excluded(far_ptr, far_idx, ii.z, sh_jtg[warp][t].y);
                   }
-                  if (excl) continue;
-                  float2 cc = make_float2(0.0f, 0.0f);
-                  if (vdw_on) cc = vdw_c6c12(sh_vdw, ii.x, tg.x);
-                  float u_vdw, u_elec;
-                  const float g = pair_terms(r2, (float)kCcelec * pi.w * pj.w, cc.x, cc.y, p, 0, vdw_on, u_vdw, u_elec);
-                  fx += g * dx;
-                  fy += g * dy;
-                  fz += g * dz;
-                  if (calc_energy) {
-                    ev += __float2ll_rn(u_vdw * kEnergyScale);
-                    ee += __float2ll_rn(u_elec * kEnergyScale);
-                  }
-                  if (calc_virial) {
-                    w0 -= g * dx * dx; w1 -= g * dx * dy; w2 -= g * dx * dz;
-                    w3 -= g * dy * dy; w4 -= g * dy * dz; w5 -= g * dz * dz;
-                  }
+                  if (!excl) hits |= 1u << t;
                 }
+              }
+            }
+            // compact the hits, ordered by lane (i) then j
+            const int cnt = __popc(hits);
+            int off = cnt;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+              const int v = __shfl_up_sync(0xffffffffu, off, d);
+              if (lane >= d) off += v;
+            }
+            const int total = __shfl_sync(0xffffffffu, off, 31);
+            off -= cnt;
+            for (unsigned m = hits; m; m &= m - 1u) sh_items[warp][off++] = (unsigned short)((lane << 5) | (__ffs(m) - 1));
+            __syncwarp();
+            // pair terms on full lanes
+            for (int base = 0; base < total; base += 32) {
+              const bool valid = base + lane < total;
+              const int item = valid ? sh_items[warp][base + lane] : 0;
+              const int il = valid ? item >> 5 : 32 + lane;   // invalid lanes get keys of their own
+              long long gx = 0, gy = 0, gz = 0;
+              if (valid) {
+                const int t = item & 31;
+                const float4 a = sh_ipos[warp][il];
+                const float4 pj = sh_jpos[warp][t];
+                // the pair vector in FP64 from the FP32 positions (exact), image by the FP64 box
+                double ddx = (double)a.x - (double)pj.x, ddy = (double)a.y - (double)pj.y,
+                       ddz = (double)a.z - (double)pj.z;
+                if (MINIMG) {
+                  ddx -= p.boxd[0] * rint(ddx / p.boxd[0]);
+                  ddy -= p.boxd[1] * rint(ddy / p.boxd[1]);
+                  ddz -= p.boxd[2] * rint(ddz / p.boxd[2]);
+                } else {
+                  ddx -= shx == 0.0f ? 0.0 : (shx > 0.0f ? p.boxd[0] : -p.boxd[0]);
+                  ddy -= shy == 0.0f ? 0.0 : (shy > 0.0f ? p.boxd[1] : -p.boxd[1]);
+                  ddz -= shz == 0.0f ? 0.0 : (shz > 0.0f ? p.boxd[2] : -p.boxd[2]);
+                }
+                const double r2 = ddx * ddx + ddy * ddy + ddz * ddz;
+                float2 cc = make_float2(0.0f, 0.0f);
+                if (vdw_on) cc = vdw_c6c12(sh_vdw, sh_itype[warp][il], sh_jtg[warp][t].x);
+                double u_vdw, u_elec;
+                const double g = pair_terms_f64(r2, kCcelec * (double)a.w * (double)pj.w, cc.x, cc.y, p, vdw_on,
+                                                u_vdw, u_elec);
+                const double fxd = g * ddx, fyd = g * ddy, fzd = g * ddz;
+                gx = __double2ll_rn(fxd * 1099511627776.0);
+                gy = __double2ll_rn(fyd * 1099511627776.0);
+                gz = __double2ll_rn(fzd * 1099511627776.0);
+                if (calc_energy) {
+                  ev += __double2ll_rn(u_vdw * 4294967296.0);
+                  ee += __double2ll_rn(u_elec * 4294967296.0);
+                }
+                if (calc_virial) {
+                  w0 -= fxd * ddx; w1 -= fxd * ddy; w2 -= fxd * ddz;
+                  w3 -= fyd * ddy; w4 -= fyd * ddz; w5 -= fzd * ddz;
+                }
+              }
+              // segmented inclusive scan over runs of equal il (int64: exact), then one add per run
+#pragma unroll
+              for (int d = 1; d < 32; d <<= 1) {
+                const int ku = __shfl_up_sync(0xffffffffu, il, d);
+                const long long ux = __shfl_up_sync(0xffffffffu, gx, d);
+                const long long uy = __shfl_up_sync(0xffffffffu, gy, d);
+                const long long uz = __shfl_up_sync(0xffffffffu, gz, d);
+                if (lane >= d && ku == il) { gx += ux; gy += uy; gz += uz; }
+              }
+              const int kn = __shfl_down_sync(0xffffffffu, il, 1);
+              if (valid && (lane == 31 || kn != il)) {
+                sh_f[warp][0][il] += gx;
+                sh_f[warp][1][il] += gy;
+                sh_f[warp][2][il] += gz;
               }
               __syncwarp();
             }
@@ -258,26 +415,27 @@ __global__ void __launch_bounds__(kWarps * 32) k_direct_pairs(
       }
       if (act) {
         const int a = ii.z;
-        atomicAdd((unsigned long long*)&force[a], (unsigned long long)__float2ll_rn(fx * kForceScaleF));
-        atomicAdd((unsigned long long*)&force[a + stride], (unsigned long long)__float2ll_rn(fy * kForceScaleF));
-        atomicAdd((unsigned long long*)&force[a + 2 * (size_t)stride], (unsigned long long)__float2ll_rn(fz * kForceScaleF));
+        atomicAdd((unsigned long long*)&force[a], (unsigned long long)sh_f[warp][0][lane]);
+        atomicAdd((unsigned long long*)&force[a + stride], (unsigned long long)sh_f[warp][1][lane]);
+        atomicAdd((unsigned long long*)&force[a + 2 * (size_t)stride], (unsigned long long)sh_f[warp][2][lane]);
       }
-      if (calc_energy) {
-        ev = warp_sum_ll(ev);
-        ee = warp_sum_ll(ee);
-        if (lane == 0) {
-          atomicAdd((unsigned long long*)&acc[kAccVdw], (unsigned long long)ev);
-          atomicAdd((unsigned long long*)&acc[kAccElec], (unsigned long long)ee);
-        }
-      }
-      if (calc_virial) {
-        const float wv[6] = {w0, w1, w2, w3, w4, w5};
+      __syncwarp();
+    }
+  }
+  if (calc_energy) {
+    ev = warp_sum_ll(ev);
+    ee = warp_sum_ll(ee);
+    if (lane == 0) {
+      atomicAdd((unsigned long long*)&acc[kAccVdw], (unsigned long long)ev);
+      atomicAdd((unsigned long long*)&acc[kAccElec], (unsigned long long)ee);
+    }
+  }
+  if (calc_virial) {
+    const double wv[6] = {w0, w1, w2, w3, w4, w5};
 #pragma unroll
-        for (int q = 0; q < 6; q++) {
-          const long long s = warp_sum_ll(__float2ll_rn(wv[q] * kEnergyScale));
-          if (lane == 0) atomicAdd((unsigned long long*)&acc[kAccVir + q], (unsigned long long)s);
-        }
-      }
+    for (int q = 0; q < 6; q++) {
+      const long long sv = warp_sum_ll(__double2ll_rn(wv[q] * 4294967296.0));
+      if (lane == 0) atomicAdd((unsigned long long*)&acc[kAccVir + q], (unsigned long long)sv);
     }
   }
 }
@@ -420,7 +578,7 @@ Params make_params(const pme_direct* h) {
   p.elec = h->elec_model;
   // cells >= roff along x (offsets -1..1) and >= roff / 2 along y and z (offsets -2..2); an axis
   // with too few cells for distinct offsets visits each of its cells once
-  const double size[3] = {h->roff, 0.5 * h->roff, 0.5 * h->roff};
+  const double size[3] = {h->roff * (1.0 + 1e-5), 0.5 * h->roff * (1.0 + 1e-5), 0.5 * h->roff * (1.0 + 1e-5)};
   const int reach[3] = {1, 2, 2};
   for (int d = 0; d < 3; d++) {
     p.nc[d] = std::max(1, (int)std::floor(h->box[d] / size[d]));
@@ -433,6 +591,11 @@ Params make_params(const pme_direct* h) {
     }
   }
   p.npair = h->npair;
+  p.kappad = h->kappa;
+  for (int d = 0; d < 3; d++) p.boxd[d] = h->box[d];
+  p.ro6d = std::pow(h->roff, -6.0);
+  p.ro12d = std::pow(h->roff, -12.0);
+  p.ro18d = std::pow(h->roff, -18.0);
   return p;
 }
 
@@ -455,7 +618,7 @@ int ensure_work(pme_direct* h, int n, int ncell) {
     h->d_count = h->d_start = nullptr;
     h->cap_cells = 0;
     if (cudaMalloc(&h->d_count, 2 * (size_t)ncell * sizeof(int)) != cudaSuccess ||
-        cudaMalloc(&h->d_start, ((size_t)ncell + 1) * sizeof(int)) != cudaSuccess) {
+        cudaMalloc(&h->d_start, 2 * ((size_t)ncell + 1) * sizeof(int)) != cudaSuccess) {
       cudaGetLastError();
       return fail(PME_ENOMEM, "direct: cell work space");
     }
@@ -698,23 +861,27 @@ int pme_direct_calc_force(pme_direct* h, const void* xyzq, int ncoord, int calc_
   if (e != cudaSuccess) return cuda_fail(e, "direct: clear counts");
   const int nb = (ncoord + 255) / 256;
   k_direct_cell<<<nb, 256, 0, s>>>((const float4*)xyzq, ncoord, p, h->d_cell_of, h->d_count);
-  k_direct_scan<<<1, 1024, 0, s>>>(h->d_count, ncell, h->d_start);
+  k_direct_scan<<<1, 1024, 0, s>>>(h->d_count, ncell, h->d_start, h->d_start + ncell + 1);
   k_direct_fill<<<nb, 256, 0, s>>>(h->d_cell_of, ncoord, h->d_start, h->d_count + ncell, h->d_tmp);
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
   const int og = std::min((ncell + 7) / 8, sms * 16);
   k_direct_order<<<og, 256, 0, s>>>(h->d_start, ncell, h->d_tmp, (const float4*)xyzq, h->d_vdwtype, h->d_glob,
-                                    h->d_win, h->d_far_ptr, h->d_pos, h->d_info, h->d_mask);
+                                    h->d_win, h->d_far_ptr, p.box[0], p.box[1], p.box[2], p.inv_box[0],
+                                    p.inv_box[1], p.inv_box[2], h->d_pos, h->d_info, h->d_mask);
+  // neighbour cells by periodic shift when every axis has distinct offsets, else minimum image
+  const bool minimg = p.cnt[0] == p.nc[0] || p.cnt[1] == p.nc[1] || p.cnt[2] == p.nc[2];
+  auto kern = minimg ? k_direct_pairs<true> : k_direct_pairs<false>;
   const size_t smem = (size_t)std::max(p.npair, 1) * sizeof(float2);
-  if (smem > 48 * 1024) {
-    e = cudaFuncSetAttribute(k_direct_pairs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return cuda_fail(e, "direct: shared memory");
-  }
-  const int tasks = ncell * kChunkStride;
-  const int pg = std::max(1, std::min((tasks + kWarps - 1) / kWarps, sms * 8));
-  k_direct_pairs<<<pg, kWarps * 32, smem, s>>>(p, h->d_start, h->d_pos, h->d_info, h->d_mask, h->d_far_ptr,
-                                               h->d_far_idx, h->d_vdw, calc_energy ? 1 : 0, calc_virial ? 1 : 0,
-                                               stride, force, h->d_acc);
+  e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(smem, 48 * 1024));
+  if (e != cudaSuccess) return cuda_fail(e, "direct: shared memory");
+  // chunks are counted on the device: enough CTAs for every (chunk, z slice) task of a uniform
+  // system, each warp striding over the rest
+  const long long tasks = (long long)((ncoord + 31) / 32 + ncell) * p.cnt[2];
+  const int pg = (int)std::max<long long>(1, std::min<long long>((tasks + kWarps - 1) / kWarps, (long long)sms * 12));
+  kern<<<pg, kWarps * 32, smem, s>>>(p, h->d_start, h->d_start + ncell + 1, h->d_pos, h->d_info, h->d_mask,
+                                     h->d_far_ptr, h->d_far_idx, h->d_vdw, calc_energy ? 1 : 0, calc_virial ? 1 : 0,
+                                     stride, force, h->d_acc);
   e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "direct: launch");
   return PME_OK;
