@@ -38,6 +38,8 @@ constexpr int kMaxTypes = 200;        // vdW types (packed pairs held in shared 
 constexpr float kEnergyScale = 4294967296.0f;     // 2^32
 constexpr float kForceScaleF = 1099511627776.0f;  // 2^40
 constexpr float kTwoSqrtPi = 1.1283791670955126f; // 2/sqrt(pi)
+constexpr int kTabN = 4096;          // Ewald table intervals
+constexpr double kTabR0 = 1.5;       // Ewald table from r = 1.5 A (closer pairs use erfc and exp)
 
 struct Params {
   float box[3], inv_box[3];
@@ -49,6 +51,11 @@ struct Params {
   int npair;          // vdW type pairs
   double kappad, ro6d, ro12d, ro18d;   // FP64 copies for the main-list pair terms
   double boxd[3];
+  // Ewald real-space table (Hermite cubic in s = r^2 on [tab_s0, roff^2], tab_n intervals):
+  // per node (E, h dE/ds, F, h dF/ds) with E = erfc(kappa r)/r and F = (r dE/dr) / r^2
+  const double4* tab;
+  double tab_s0, tab_invh;
+  int tab_n;
 };
 
 enum Acc { kAccVdw = 0, kAccElec = 1, kAccExcl = 2, kAccVir = 3, kAccN = 9 };   // vir: xx xy xz yy yz zz
@@ -93,6 +100,18 @@ __device__ __forceinline__ double pair_terms_f64(double r2, double qq, double c6
     fr = c6 * (rinv6 - r6 * p.ro12d) - c12 * (rinv12 + r6 * p.ro18d);
     u_vdw = c12 * (1.0 / 12.0) * (rinv12 + 2.0 * r6 * p.ro18d - 3.0 * p.ro12d) -
             c6 * (1.0 / 6.0) * (rinv6 + r6 * p.ro12d - 2.0 * p.ro6d);
+  }
+  if (p.tab != nullptr && r2 >= p.tab_s0) {
+    const double u = (r2 - p.tab_s0) * p.tab_invh;
+    const int i = min((int)u, p.tab_n - 1);
+    const double t = u - (double)i;
+    const double2* q = reinterpret_cast<const double2*>(p.tab + i);
+    const double2 a0 = __ldg(q), a1 = __ldg(q + 1), b0 = __ldg(q + 2), b1 = __ldg(q + 3);
+    const double t2 = t * t;
+    const double h01 = t2 * (3.0 - 2.0 * t), h00 = 1.0 - h01;
+    const double h10 = t * (1.0 - t) * (1.0 - t), h11 = t2 * (t - 1.0);
+    u_elec = qq * (h00 * a0.x + h10 * a0.y + h01 * b0.x + h11 * b0.y);
+    return fr * rinv2 + qq * (h00 * a1.x + h10 * a1.y + h01 * b1.x + h11 * b1.y);
   }
   const double e = qq * erfc(p.kappad * r) * rinv;
   u_elec = e;
@@ -237,7 +256,7 @@ __global__ void __launch_bounds__(kWarps * 32, 3) k_direct_pairs(
     const int4* __restrict__ info,
     const ulonglong2* __restrict__ mask, const int* __restrict__ far_ptr, const int* __restrict__ far_idx,
     const float2* __restrict__ vdwp, int calc_energy, int calc_virial, int stride, long long* __restrict__ force,
-    long long* __restrict__ acc) {
+    long long* __restrict__ acc, int* __restrict__ next_task) {
   extern __shared__ float2 sh_vdw[];
   __shared__ float4 sh_jpos[kWarps][32];
   __shared__ int2 sh_jtg[kWarps][32];
@@ -252,10 +271,15 @@ __global__ void __launch_bounds__(kWarps * 32, 3) k_direct_pairs(
   const int nslice = p.cnt[2];
   const bool vdw_on = p.vdw != PME_VDW_NONE;
   long long ev = 0, ee = 0;
-  double w0 = 0.0, w1 = 0.0, w2 = 0.0, w3 = 0.0, w4 = 0.0, w5 = 0.0;
+  long long wv[6] = {0, 0, 0, 0, 0, 0};   // virial at 2^32: each task's FP64 partials folded in (exact)
   const int nchunk = chunkp[ncell];
   const int ntask = nchunk * nslice;
-  for (int task = blockIdx.x * kWarps + warp; task < ntask; task += gridDim.x * kWarps) {
+  // tasks differ in cost (cell populations): warps take them one at a time from a counter
+  for (;;) {
+    int task = 0;
+    if (lane == 0) task = atomicAdd(next_task, 1);
+    task = __shfl_sync(0xffffffffu, task, 0);
+    if (task >= ntask) break;
     const int sl = task % nslice;
     const int g = task / nslice;
     int clo = 0, chi = ncell - 1;   // the cell holding chunk g: last c with chunkp[c] <= g
@@ -266,6 +290,7 @@ __global__ void __launch_bounds__(kWarps * 32, 3) k_direct_pairs(
     const int c = clo;
     const int ce = start[c + 1];
     const int cx = c % p.nc[0], cy = (c / p.nc[0]) % p.nc[1], cz = c / (p.nc[0] * p.nc[1]);
+    double w0 = 0.0, w1 = 0.0, w2 = 0.0, w3 = 0.0, w4 = 0.0, w5 = 0.0;   // this task's, in a fixed order
     {
       const int chunk = start[c] + (g - chunkp[c]) * 32;
       const int i = chunk + lane;
@@ -421,6 +446,11 @@ __global__ void __launch_bounds__(kWarps * 32, 3) k_direct_pairs(
       }
       __syncwarp();
     }
+    if (calc_virial) {
+      wv[0] += __double2ll_rn(w0 * 4294967296.0); wv[1] += __double2ll_rn(w1 * 4294967296.0);
+      wv[2] += __double2ll_rn(w2 * 4294967296.0); wv[3] += __double2ll_rn(w3 * 4294967296.0);
+      wv[4] += __double2ll_rn(w4 * 4294967296.0); wv[5] += __double2ll_rn(w5 * 4294967296.0);
+    }
   }
   if (calc_energy) {
     ev = warp_sum_ll(ev);
@@ -431,10 +461,9 @@ __global__ void __launch_bounds__(kWarps * 32, 3) k_direct_pairs(
     }
   }
   if (calc_virial) {
-    const double wv[6] = {w0, w1, w2, w3, w4, w5};
 #pragma unroll
     for (int q = 0; q < 6; q++) {
-      const long long sv = warp_sum_ll(__double2ll_rn(wv[q] * 4294967296.0));
+      const long long sv = warp_sum_ll(wv[q]);
       if (lane == 0) atomicAdd((unsigned long long*)&acc[kAccVir + q], (unsigned long long)sv);
     }
   }
@@ -529,6 +558,8 @@ struct pme_direct {
   int* d_far_ptr = nullptr;
   int* d_far_idx = nullptr;
   bool excl_set = false;
+  double4* d_tab = nullptr;  // Ewald real-space table for the current kappa and roff
+  double tab_kappa = -1.0, tab_roff = -1.0;
   int4* d_list14 = nullptr;
   int n14 = 0;
   int max14 = -1;            // largest atom index in the 1-4 lists
@@ -536,7 +567,7 @@ struct pme_direct {
   int cap_atoms = 0, cap_cells = 0;
   int* d_cell_of = nullptr;
   int* d_tmp = nullptr;
-  int* d_count = nullptr;     // [cap_cells] counts, then [cap_cells] fill counters
+  int* d_count = nullptr;     // [cap_cells] counts, [cap_cells] fill counters, the pair-task counter
   int* d_start = nullptr;     // [cap_cells + 1]
   float4* d_pos = nullptr;
   int4* d_info = nullptr;
@@ -593,10 +624,45 @@ Params make_params(const pme_direct* h) {
   p.npair = h->npair;
   p.kappad = h->kappa;
   for (int d = 0; d < 3; d++) p.boxd[d] = h->box[d];
+  p.tab = h->d_tab;
+  p.tab_s0 = kTabR0 * kTabR0;
+  p.tab_invh = kTabN / (h->roff * h->roff - p.tab_s0);
+  p.tab_n = kTabN;
   p.ro6d = std::pow(h->roff, -6.0);
   p.ro12d = std::pow(h->roff, -12.0);
   p.ro18d = std::pow(h->roff, -18.0);
   return p;
+}
+
+// Hermite table of E(s) = erfc(kappa sqrt s) / sqrt s and F(s) = (r dE/dr) / r^2 (with r dE/dr =
+// -2/sqrt(pi) kappa r exp(-kappa^2 s) - E... written per qq: the pair's r dU_elec/dr / r^2), values
+// and h-scaled s-derivatives at kTabN + 1 nodes, built in FP64 on the host.  Cubic Hermite
+// interpolation of these smooth functions at this spacing is within ~1e-9 relative.
+int ensure_table(pme_direct* h) {
+  if (h->elec_model == PME_ELEC_NONE) return PME_OK;
+  if (h->d_tab && h->tab_kappa == h->kappa && h->tab_roff == h->roff) return PME_OK;
+  cudaFree(h->d_tab);
+  h->d_tab = nullptr;
+  const double s0 = kTabR0 * kTabR0, s1 = h->roff * h->roff;
+  if (!(s1 > s0)) return PME_OK;
+  const double k = h->kappa, c1 = 2.0 / std::sqrt(kPi) * k, hs = (s1 - s0) / kTabN;
+  std::vector<double4> t((size_t)kTabN + 1);
+  for (int i = 0; i <= kTabN; i++) {
+    const double sv = s0 + hs * i, r = std::sqrt(sv), ex = std::exp(-k * k * sv);
+    const double E = std::erfc(k * r) / r;
+    const double dEdr = (-c1 * ex * r - std::erfc(k * r)) / (r * r);
+    const double dEds = dEdr / (2.0 * r);
+    const double A = -c1 * ex - E;            // r dE/dr
+    const double F = A / sv;
+    const double dAds = c1 * k * k * ex - dEds;
+    const double dFds = (dAds * sv - A) / (sv * sv);
+    t[i] = make_double4(E, hs * dEds, F, hs * dFds);
+  }
+  cudaError_t e = upload(&h->d_tab, t.data(), t.size(), h->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "direct: Ewald table");
+  h->tab_kappa = h->kappa;
+  h->tab_roff = h->roff;
+  return PME_OK;
 }
 
 int ensure_work(pme_direct* h, int n, int ncell) {
@@ -617,7 +683,7 @@ int ensure_work(pme_direct* h, int n, int ncell) {
     cudaFree(h->d_count); cudaFree(h->d_start);
     h->d_count = h->d_start = nullptr;
     h->cap_cells = 0;
-    if (cudaMalloc(&h->d_count, 2 * (size_t)ncell * sizeof(int)) != cudaSuccess ||
+    if (cudaMalloc(&h->d_count, (2 * (size_t)ncell + 1) * sizeof(int)) != cudaSuccess ||
         cudaMalloc(&h->d_start, 2 * ((size_t)ncell + 1) * sizeof(int)) != cudaSuccess) {
       cudaGetLastError();
       return fail(PME_ENOMEM, "direct: cell work space");
@@ -685,7 +751,7 @@ int pme_direct_destroy(pme_direct* h) {
   DeviceGuard dg(h->device);
   cudaStreamSynchronize(h->stream);
   for (void* p : {(void*)h->d_vdw, (void*)h->d_vdw14, (void*)h->d_vdwtype, (void*)h->d_glob, (void*)h->d_win,
-                  (void*)h->d_far_ptr, (void*)h->d_far_idx, (void*)h->d_list14, (void*)h->d_cell_of, (void*)h->d_tmp,
+                  (void*)h->d_far_ptr, (void*)h->d_far_idx, (void*)h->d_list14, (void*)h->d_tab, (void*)h->d_cell_of, (void*)h->d_tmp,
                   (void*)h->d_count, (void*)h->d_start, (void*)h->d_pos, (void*)h->d_info, (void*)h->d_mask,
                   (void*)h->d_acc})
     if (p) cudaFree(p);
@@ -852,12 +918,13 @@ int pme_direct_calc_force(pme_direct* h, const void* xyzq, int ncoord, int calc_
     h->n_types = ncoord;
     h->max_type = 0;
   }
+  if (int rc = ensure_table(h)) return rc;
   Params p = make_params(h);
   if (h->vdw_model == PME_VDW_NONE) p.npair = 0;
   const int ncell = p.nc[0] * p.nc[1] * p.nc[2];
   if (int rc = ensure_work(h, ncoord, ncell)) return rc;
   cudaStream_t s = h->stream;
-  cudaError_t e = cudaMemsetAsync(h->d_count, 0, 2 * (size_t)ncell * sizeof(int), s);
+  cudaError_t e = cudaMemsetAsync(h->d_count, 0, (2 * (size_t)ncell + 1) * sizeof(int), s);   // + task counter
   if (e != cudaSuccess) return cuda_fail(e, "direct: clear counts");
   const int nb = (ncoord + 255) / 256;
   k_direct_cell<<<nb, 256, 0, s>>>((const float4*)xyzq, ncoord, p, h->d_cell_of, h->d_count);
@@ -877,11 +944,16 @@ int pme_direct_calc_force(pme_direct* h, const void* xyzq, int ncoord, int calc_
   if (e != cudaSuccess) return cuda_fail(e, "direct: shared memory");
   // chunks are counted on the device: enough CTAs for every (chunk, z slice) task of a uniform
   // system, each warp striding over the rest
+  // one wave of resident CTAs; their warps draw the (chunk, z slice) tasks from a counter
+  int occ = 1;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kWarps * 32, smem);
+  if (e != cudaSuccess) return cuda_fail(e, "direct: occupancy");
   const long long tasks = (long long)((ncoord + 31) / 32 + ncell) * p.cnt[2];
-  const int pg = (int)std::max<long long>(1, std::min<long long>((tasks + kWarps - 1) / kWarps, (long long)sms * 12));
+  const int pg = (int)std::max<long long>(1, std::min<long long>((tasks + kWarps - 1) / kWarps,
+                                                                 (long long)sms * std::max(occ, 1)));
   kern<<<pg, kWarps * 32, smem, s>>>(p, h->d_start, h->d_start + ncell + 1, h->d_pos, h->d_info, h->d_mask,
                                      h->d_far_ptr, h->d_far_idx, h->d_vdw, calc_energy ? 1 : 0, calc_virial ? 1 : 0,
-                                     stride, force, h->d_acc);
+                                     stride, force, h->d_acc, h->d_count + 2 * ncell);
   e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "direct: launch");
   return PME_OK;

@@ -12,11 +12,11 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 CUDA = "/usr/local/cuda"
 
 
-def _build(tmp):
+def _build(tmp, name="recip_driver"):
     from gpu_recip_b200 import build
     lib = build.build()
-    exe = os.path.join(tmp, "recip_driver")
-    cmd = ["g++", "-std=c++17", "-O2", os.path.join(ROOT, "tests", "cpp", "recip_driver.cpp"),
+    exe = os.path.join(tmp, name)
+    cmd = ["g++", "-std=c++17", "-O2", os.path.join(ROOT, "tests", "cpp", name + ".cpp"),
            "-I", os.path.join(ROOT, "include"), "-I", os.path.join(CUDA, "include"),
            "-L", os.path.dirname(lib), "-lpme_b200", "-L", os.path.join(CUDA, "lib64"), "-lcudart",
            "-Wl,-rpath," + os.path.dirname(lib), "-Wl,-rpath," + os.path.join(CUDA, "lib64"), "-o", exe]
@@ -24,10 +24,11 @@ def _build(tmp):
     return exe
 
 
-def test_cpp_driver_compiles_against_the_header():
+@pytest.mark.parametrize("name", ["recip_driver", "direct_driver"])
+def test_cpp_driver_compiles_against_the_header(name):
     with tempfile.TemporaryDirectory() as tmp:
         obj = os.path.join(tmp, "d.o")
-        subprocess.run(["g++", "-std=c++17", "-c", os.path.join(ROOT, "tests", "cpp", "recip_driver.cpp"),
+        subprocess.run(["g++", "-std=c++17", "-c", os.path.join(ROOT, "tests", "cpp", name + ".cpp"),
                         "-I", os.path.join(ROOT, "include"), "-I", os.path.join(CUDA, "include"), "-o", obj],
                        check=True)
         assert os.path.getsize(obj) > 0
@@ -61,3 +62,34 @@ def test_cpp_driver_on_reference_fixture(cuda, ref_fixture, order):
     assert abs(e0 - f[f"energy{order}"]) < f[f"tol_energy{order}"]
     assert np.abs(v0 - f[f"virial{order}"]).max() < f[f"tol_virial{order}"]
     assert np.abs(f0 - f[f"force{order}"]).max() < f[f"tol_force{order}"]
+
+
+@pytest.mark.gpu
+def test_cpp_direct_driver_on_reference_fixture(cuda):
+    """The reference's direct test sequence from C++ (gpu_direct.cu:151-233) on its own fixture:
+    main-list forces, energies and virial, then the total with the 1-4 lists, within the driver's
+    tolerances."""
+    from tests.conftest import GOLDEN
+    d = dict(np.load(os.path.join(GOLDEN, "ref_direct_23558.npz")))
+    n = d["xyzq"].shape[0]
+    with tempfile.TemporaryDirectory() as tmp:
+        exe = _build(tmp, "direct_driver")
+        inp, out = os.path.join(tmp, "in.bin"), os.path.join(tmp, "out.bin")
+        with open(inp, "wb") as fh:
+            fh.write(np.array([n, d["vdwparam"].size, d["vdwparam14"].size, d["in14"].shape[0],
+                               d["ex14"].shape[0], d["inb14"].size], np.int32).tobytes())
+            fh.write(np.array([*d["box"], float(d["kappa"]), float(d["roff"]), float(d["ron"]),
+                               float(d["e14fac"])], np.float64).tobytes())
+            fh.write(np.ascontiguousarray(d["xyzq"], np.float32).tobytes())
+            fh.write(d["vdwparam"].astype(np.float32).tobytes())
+            fh.write(d["vdwparam14"].astype(np.float32).tobytes())
+            for key in ("vdwtype", "iblo14", "inb14", "loc2glo", "in14", "ex14"):
+                fh.write(np.ascontiguousarray(d[key], np.int32).tobytes())
+        subprocess.run([exe, inp, out], check=True, timeout=120)
+        raw = np.fromfile(out, dtype=np.float64)
+    per = 12 + 3 * n
+    main, total = raw[:per], raw[per:2 * per]
+    assert np.abs(main[12:].reshape(n, 3) - d["force_main"]).max() <= d["tol_force_main"]
+    assert abs(main[0] - d["energy_vdw"]) < d["tol_energy"] and abs(main[1] - d["energy_elec"]) < d["tol_energy"]
+    assert np.abs(main[3:12].reshape(3, 3) - d["virial"]).max() < d["tol_virial"]
+    assert np.abs(total[12:].reshape(n, 3) - d["force_total"]).max() <= d["tol_force_total"]
