@@ -9,7 +9,8 @@ atoms) in a 62.1 A cube, 64^3 grid, spline order 4, kappa 0.32 (seeded synthetic
 
 value: device-timed evals/s with inputs resident in HBM, L2 flushed (256 MiB write) before every
 step outside the per-step CUDA-event pair.  e2e: the same through the C ABI with host buffers:
-pinned xyzq H2D, evaluation, forces + energy/virial D2H, all inside the timed region.
+pinned xyzq H2D, evaluation, forces D2H and the energy/virial record into pinned host memory
+(written by the kernel through the record mirror), all inside the timed region.
 roofline: the dominant stage of the staged C-ABI calls, timed with CUDA events on the
 operator's stream, algorithmic bytes per launch against the measured HBM copy bandwidth.
 --impl reference: the CPU oracle (multithreaded FP64 restatement of the reference algorithm;
@@ -275,19 +276,23 @@ def run_b200(args):
     e_starts = [torch.cuda.Event(enable_timing=True) for _ in range(Ke)]
     e_ends = [torch.cuda.Event(enable_timing=True) for _ in range(Ke)]
     x_in = torch.empty_like(x_dev)
+    # the step's energy and virial reach pinned host memory from the kernel itself (the record
+    # mirror): per step one copy in, the evaluation, one copy of the forces out
+    pme.set_energy_virial_mirror(ev_host)
     with torch.cuda.stream(stream):
         for i in range(Ke + 3):
             flush.fill_(0.0)
             if i >= 3:
                 e_starts[i - 3].record(stream)
             x_in.copy_(x_host, non_blocking=True)
-            pme.energy_virial.clear()
             pme.eval_ortho(inv_box, x_in, n, s.kappa, True, True, f_dev, stride)
             f_host.copy_(f_dev, non_blocking=True)
-            pme.energy_virial.copy_async(ev_host)
             if i >= 3:
                 e_ends[i - 3].record(stream)
     stream.synchronize()
+    pme.set_energy_virial_mirror(None)
+    if not np.isfinite(ev_host.numpy()).all() or ev_host[0].item() == 0.0:
+        raise RuntimeError("e2e: the energy record did not reach the host")
     e_total = R.max_over_ranks(float(sum(e_starts[i].elapsed_time(e_ends[i]) for i in range(Ke))), dev)
     e2e_value = R.aggregate_rate([Ke] * world, e_total / 1000.0)
 

@@ -49,6 +49,7 @@ SIGNATURES = {
     "pme_get_energy_virial": [_P, _DP, _DP, _DP],
     "pme_copy_energy_virial_async": [_P, _P],
     "pme_energy_virial_device_ptr": [_P, ctypes.POINTER(_P)],
+    "pme_set_energy_virial_mirror": [_P, _P],
     "pme_eval_ortho": [_P, _D, _D, _D, _P, _I, _D, _I, _I, _I, _P, _I],
     "pme_eval": [_P, _DP, _P, _I, _D, _I, _I, _I, _P, _I],
     "pme_copy_charge_grid_fixed": [_P, _P],

@@ -51,6 +51,7 @@ struct pme_recip {
   int inject = 0;
   unsigned long long* trace = nullptr;
   int trace_ctas = 0;
+  double* ev_mirror = nullptr;   // device-mapped pinned host memory, or null
   int plane_mode = 0;   // 0 automatic, 1 whole-plane tiles where they fit, 2 separate passes
   int grid_cap = 0;     // CTAs of the persistent launch (0: as many as are resident)
 };
@@ -398,6 +399,20 @@ int pme_energy_virial_device_ptr(pme_recip* h, double** dev_ptr) {
   return PME_OK;
 }
 
+int pme_set_energy_virial_mirror(pme_recip* h, double* host_mapped) {
+  if (int rc = handle_ok(h)) return rc;
+  if (host_mapped) {
+    cudaPointerAttributes a;
+    cudaError_t e = cudaPointerGetAttributes(&a, host_mapped);
+    if (e != cudaSuccess || a.type != cudaMemoryTypeHost || a.devicePointer != (void*)host_mapped) {
+      cudaGetLastError();
+      return fail(PME_EINVAL, "energy/virial mirror must be pinned host memory mapped at the same address");
+    }
+  }
+  h->ev_mirror = host_mapped;
+  return PME_OK;
+}
+
 int pme_eval_ortho(pme_recip* h, double inv_boxx, double inv_boxy, double inv_boxz, const void* xyzq,
                    int ncoord, double kappa, int calc_energy, int calc_virial, int kind, void* force,
                    int stride) {
@@ -421,6 +436,7 @@ int pme_eval(pme_recip* h, const double* recip, const void* xyzq, int ncoord, do
   if (int rc = ensure_bins(h, ncoord)) return rc;
   const int ev = (calc_energy || calc_virial) ? 1 : 0;
   SysDesc d = h->st.desc9(recip, kappa, xyzq, ncoord, force, kind, stride, ev, calc_energy ? 1 : 0);
+  d.ev_mirror = h->ev_mirror;
   return launch_fused_single(h, d);
 }
 

@@ -60,6 +60,7 @@ struct SysDesc {
   const float2* tw;          // twiddles x | y | z (plan.tw_off)
   long long* acc;            // kAccCount fixed-point accumulators
   double* ev;                // kEvCount record
+  double* ev_mirror;         // optional device-mapped host copy of each evaluation's own record
   int tx_rows, tx_y, tx_z;   // lines per tile of the x, y, z passes
   int plane;                 // 1: the fused path runs y, z and the solve as whole-plane tiles
   // Atom bins of the fused path: bin (by, bz) holds the atoms whose stencil origin (iy0, iz0)
@@ -1144,9 +1145,13 @@ __device__ __forceinline__ void spread_x_dispatch(const SysDesc& d, int tile, in
 }
 
 // Convert the accumulators into the FP64 record and clear them (one thread).
+// With a mirror (fused evaluations only: solve and self together) this evaluation's own record is
+// also stored there, zeros for the terms not asked for.
 __device__ __forceinline__ void finalize_system(const SysDesc& d, bool solve, bool self) {
   long long* acc = d.acc;
   double* ev = d.ev;
+  double own[kEvCount];
+  for (int c = 0; c < kEvCount; c++) own[c] = 0.0;
   if (solve && d.calc_ev) {
     double s[7];
     for (int c = 0; c < 7; c++) {
@@ -1154,17 +1159,22 @@ __device__ __forceinline__ void finalize_system(const SysDesc& d, bool solve, bo
       acc[kAccE + c] = 0;
     }
     const double h = 0.5 * kCcelec;
-    ev[kEvRecip] += h * s[0];
-    double* vir = ev + kEvVirial;
-    vir[0] -= h * s[1]; vir[1] -= h * s[2]; vir[2] -= h * s[3];
-    vir[3] -= h * s[2]; vir[4] -= h * s[4]; vir[5] -= h * s[5];
-    vir[6] -= h * s[3]; vir[7] -= h * s[5]; vir[8] -= h * s[6];
+    own[kEvRecip] = h * s[0];
+    double* vir = own + kEvVirial;
+    vir[0] = -h * s[1]; vir[1] = -h * s[2]; vir[2] = -h * s[3];
+    vir[3] = -h * s[2]; vir[4] = -h * s[4]; vir[5] = -h * s[5];
+    vir[6] = -h * s[3]; vir[7] = -h * s[5]; vir[8] = -h * s[6];
+    ev[kEvRecip] += own[kEvRecip];
+    for (int c = 0; c < 9; c++) ev[kEvVirial + c] += vir[c];
   }
   if (self && d.calc_self) {
     const double q2 = (double)acc[kAccQ2] / kQ2Scale;
     acc[kAccQ2] = 0;
-    ev[kEvSelf] += d.self_coef * q2;
+    own[kEvSelf] = d.self_coef * q2;
+    ev[kEvSelf] += own[kEvSelf];
   }
+  if (d.ev_mirror != nullptr && solve && self)
+    for (int c = 0; c < kEvCount; c++) d.ev_mirror[c] = own[c];
 }
 
 // ---------------------------------------------------------------------------------------------

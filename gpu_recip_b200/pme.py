@@ -217,6 +217,15 @@ class CudaPMERecip:
                 "calc_self_energy")
 
     # -- fused evaluation (CudaDomdecRecip::calc) -----------------------------------------------
+    def set_energy_virial_mirror(self, host_tensor=None):
+        """Each later fused evaluation also writes its own [E_recip, E_self, W(9)] record into
+        ``host_tensor`` (a pinned float64 CPU tensor of 11 values), or stop with None."""
+        if host_tensor is not None and (host_tensor.numel() < 11 or not host_tensor.is_pinned()):
+            raise ValueError("the mirror must be a pinned tensor of at least 11 float64 values")
+        self._mirror = host_tensor   # keep it alive
+        ptr = None if host_tensor is None else ctypes.c_void_p(host_tensor.data_ptr())
+        C.check(self._lib.pme_set_energy_virial_mirror(self._h, ptr), "set_energy_virial_mirror")
+
     def eval(self, recip, xyzq, ncoord: int, kappa: float, calc_energy: bool, calc_virial: bool,
              force, stride: int = 0, kind: Optional[int] = None):
         """Fused evaluation for any box (pme_eval): recip is the row-major reciprocal matrix,

@@ -95,6 +95,12 @@ PME_API int pme_get_energy_virial(pme_recip* h, double* energy_recip, double* en
 PME_API int pme_copy_energy_virial_async(pme_recip* h, double* dst);
 /* Device address of the record: double[PME_EV_COUNT]. */
 PME_API int pme_energy_virial_device_ptr(pme_recip* h, double** dev_ptr);
+/* Opt-in (no counterpart in the reference): every later fused evaluation (pme_eval,
+ * pme_eval_ortho) also stores its own record [E_recip, E_self, W_xx .. W_zz] (not the accumulated
+ * one; zeros for terms not asked for) at host_mapped, pinned host memory mapped at the same
+ * address (cudaHostAlloc / cudaMallocHost with unified addressing), readable once the stream has
+ * passed the evaluation.  The device record accumulates as before.  NULL turns it off. */
+PME_API int pme_set_energy_virial_mirror(pme_recip* h, double* host_mapped);
 
 /* ---- fused evaluation: the CudaDomdecRecip::calc sequence (CudaDomdecRecip.h:17-81) ----
  * spread, R2C, scalar sum (energy/virial if asked), C2R, gather into `force` of `kind`, and the

@@ -1,6 +1,7 @@
 """The MD-side callers of the path: CudaDomdecRecip::calc with its three force outputs
 (CudaDomdecRecip.h:50-81), the int64 output accumulating onto forces already there (as direct-space
 forces would be), and the recip node's request loop (CudaDomdecRecipLooper::run) in process."""
+import ctypes
 import threading
 
 import numpy as np
@@ -77,3 +78,39 @@ def test_recip_looper_serves_a_direct_node(cuda):
         comm.send_stop()
         th.join(timeout=120)
     assert not th.is_alive() and out["steps"] == 3
+
+
+def test_energy_virial_mirror_holds_each_evaluations_own_record(cuda):
+    """pme_set_energy_virial_mirror: each fused evaluation writes its own record to pinned host
+    memory while the device record keeps accumulating."""
+    torch = cuda
+    from gpu_recip_b200 import CudaPMERecip, _capi, force_stride
+    s = S.config_small(seed=12)
+    pme = CudaPMERecip(*s.nfft, s.order)
+    x = torch.from_numpy(s.xyzq).cuda()
+    st = force_stride(s.natom)
+    f = torch.zeros(3 * st, dtype=torch.float32, device="cuda")
+    inv = [1.0 / b for b in s.box]
+    mirror = torch.zeros(11, dtype=torch.float64).pin_memory()
+    pme.set_energy_virial_mirror(mirror)
+    ev = pme.energy_virial
+    ev.clear()
+    pme.eval_ortho(inv, x, s.natom, s.kappa, True, True, f, st)
+    torch.cuda.synchronize()
+    first = mirror.numpy().copy()
+    ev.copyToHost()
+    assert first[0] == ev.getEnergy("recip") and first[1] == ev.getEnergy("self")
+    assert np.array_equal(first[2:].reshape(3, 3), ev.getVirial())
+    pme.eval_ortho(inv, x, s.natom, s.kappa, True, True, f, st)   # no clear: the record doubles
+    torch.cuda.synchronize()
+    ev.copyToHost()
+    assert np.array_equal(mirror.numpy(), first)
+    assert ev.getEnergy("recip") == 2 * first[0]
+    pme.eval_ortho(inv, x, s.natom, s.kappa, False, False, f, st)   # nothing asked: zeros
+    torch.cuda.synchronize()
+    assert not mirror.numpy().any()
+    pme.set_energy_virial_mirror(None)
+    with pytest.raises(_capi.PMEError) as e:   # device memory is not a host mirror
+        _capi.check(pme._lib.pme_set_energy_virial_mirror(pme._h, ctypes.c_void_p(f.data_ptr())), "mirror")
+    assert e.value.status == _capi.PME_EINVAL
+    pme.close()
