@@ -177,7 +177,9 @@ __device__ __forceinline__ void fft_stage(const float2* __restrict__ in, float2*
 
 // Full transform of every line of the tile held in buf0 (element stride es, line stride ls);
 // returns the buffer that holds the result (buf0 or buf1).  Every thread of the CTA must call
-// it; it synchronises between stages and before returning.
+// it; it synchronises between stages and before returning.  Not inlined: the fused evaluation
+// runs it in five phases, and one shared copy of its stages is what those phases fetch (with L2
+// cold, per-phase inlined copies cost ~15 us of instruction fetch per evaluation).
 static __device__ __noinline__ float2* fft_tile(float2* buf0, float2* buf1, const FftPlan1D& plan,
                                          int es, int ls, const TileLane ln, const float2* tw,
                                          bool inv) {

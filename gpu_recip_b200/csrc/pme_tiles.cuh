@@ -56,7 +56,7 @@ struct SysDesc {
   float2* cgrid;             // half-complex grid [z][y][kx]
   float* rgrid;              // solved real grid [z][y][x]
   const double* bmod;        // B-spline moduli 1/|b|^2, x | y | z (FP64)
-  double* ktab;              // influence tables: mhat x|y|z, then A = bmod exp(-fac mhat^2) x|y|z
+  double* ktab;              // influence tables, 4 rows of nx+ny+nz (see ktab_tile)
   const float2* tw;          // twiddles x | y | z (plan.tw_off)
   long long* acc;            // kAccCount fixed-point accumulators
   double* ev;                // kEvCount record
