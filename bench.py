@@ -36,7 +36,7 @@ METRIC = "PME recip evals/s at 24k atoms/64^3; batched evals/s + p50/p99 latency
 
 # DRAM bytes (read + write) of one k_fused launch from an ncu capture, by workload (mean of 3
 # launches; profiles/k_fused_water8k_64_p4_full.md).  None where not captured.
-TRAFFIC_BYTES = {"water8k_64_p4": 660395}
+TRAFFIC_BYTES = {"water8k_64_p4": 659883}
 UNIT = "evals/s"
 FALLBACK_HBM_GBS = 6650.0
 
@@ -149,6 +149,33 @@ class ClockSampler:
         reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": reasons, "samples": len(rows)}
+
+
+def workload_parity(pme, s, x_dev, f_dev, stride, inv_box, stream):
+    """One fused evaluation of the workload against the FP64 oracle on the same inputs: force
+    relative RMS, energy and virial errors, and whether the int64 charge grid is bit-exact
+    against the oracle's FP32 mirror (tolerances: force 1e-5, energy 1e-6)."""
+    import torch
+    from oracle import oracle as O
+    O.build()
+    n = s.natom
+    with torch.cuda.stream(stream):
+        pme.energy_virial.clear()
+        pme.eval_ortho(inv_box, x_dev, n, s.kappa, True, True, f_dev, stride)
+    stream.synchronize()
+    ev = pme.energy_virial
+    ev.copyToHost()
+    f = f_dev.view(3, stride)[:, :n].T.cpu().numpy().astype(np.float64)
+    ref = O.evaluate(s.xyzq.astype(np.float64), s.recip3, s.nfft, s.order, s.kappa)
+    pme.spread_charge(x_dev, n, [inv_box[0], 0, 0, 0, inv_box[1], 0, 0, 0, inv_box[2]])
+    grid_exact = bool(np.array_equal(pme.charge_grid_fixed(), O.spread_fixed(s.xyzq, s.recip3, s.nfft, s.order)))
+    return {"vs": "FP64 oracle (CPU) on the same inputs",
+            "force_rel_rms": float(np.sqrt(((f - ref["force"]) ** 2).sum() / (ref["force"] ** 2).sum())),
+            "energy_rel": float(abs(ev.getEnergy("recip") - ref["energy"]) / abs(ref["energy"])),
+            "self_energy_rel": float(abs(ev.getEnergy("self") - ref["energy_self"]) / abs(ref["energy_self"])),
+            "virial_rel": float(np.abs(ev.getVirial() - ref["virial"]).max() / np.abs(ref["virial"]).max()),
+            "charge_grid_bit_exact": grid_exact,
+            "tolerances": {"force_rel_rms": 1e-5, "energy_rel": 1e-6}}
 
 
 def cpu_oracle_rate(s, seconds: float, nthreads: int = 0):
@@ -311,6 +338,7 @@ def run_b200(args):
 
     fft_cmp = fft_comparator(s, stages, dev)
 
+
     # ---- batched: uneven systems in one persistent launch --------------------------------------------
     batched = None
     if args.batch > 0:
@@ -340,7 +368,9 @@ def run_b200(args):
     if rank == 0 and not args.no_cpu_baseline:
         rate, cnt, dt, cores = cpu_oracle_rate(s, args.cpu_seconds)
         cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
-               "sample": f"{cnt} full FP64 evaluations of the workload ({dt:.1f} s)"}
+               "sample": f"{cnt} full FP64 evaluations of the workload ({dt:.1f} s)",
+               # the same FP64 evaluation checks the GPU's result on these inputs
+               "gpu_parity": workload_parity(pme, s, x_dev, f_dev, stride, inv_box, stream)}
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
