@@ -179,3 +179,25 @@ def test_direct_argument_checks(cuda):
         dr.set_exclusions([1, 1, 1, 1], [2], [0, 0, 1, 2])
     assert e.value.status == _capi.PME_EINVAL
     dr.close()
+
+
+@pytest.mark.parametrize("box,n", [(20.0, 3000), (40.0, 24000)])   # every axis with too few cells; shifts
+def test_direct_dense_cells_many_chunks(cuda, oracle, box, n):
+    """About 90 atoms per cell (three 32-atom chunks each): electrostatics only (random charges
+    closer than any vdW model would allow), against the FP64 oracle."""
+    from gpu_recip_b200.direct import CudaPMEDirectForce, EWALD, VDW_NONE
+    rng = np.random.default_rng(n)
+    x = np.empty((n, 4), np.float32)
+    x[:, :3] = rng.random((n, 3)) * box
+    x[:, 3] = rng.normal(0.0, 0.3, n)
+    dr = CudaPMEDirectForce()
+    dr.setup(box, box, box, 0.35, 9.0, 7.5, 1.0, VDW_NONE, EWALD)
+    xd = cuda.from_numpy(x).cuda()
+    fi, e, vir = _run(cuda, dr, xd, n, n)
+    fo, _, ee, vo = oracle.direct_force(x.astype(np.float64), np.array([box] * 3), 0.35, 9.0, np.zeros(2),
+                                        np.zeros(n, np.int32), np.zeros(n + 1, np.int32), np.zeros(0, np.int32))
+    f = fi.astype(np.float64) / FORCE_SCALE
+    assert np.sqrt(((f - fo) ** 2).sum() / (fo ** 2).sum()) <= 1e-6
+    assert abs(e["elec"] - ee) <= 1e-7 * abs(ee) + 1e-6
+    assert np.abs(vir - vo).max() <= 1e-6 * np.abs(vo).max()
+    dr.close()
