@@ -77,6 +77,8 @@ __device__ __forceinline__ float pair_terms(float r2, float qq, float c6, float 
     u_vdw = c12 * (1.0f / 12.0f) * (rinv12 + 2.0f * r6 * p.ro18 - 3.0f * p.ro12) -
             c6 * (1.0f / 6.0f) * (rinv6 + r6 * p.ro12 - 2.0f * p.ro6);
   }
+  u_elec = 0.0f;
+  if (p.elec == PME_ELEC_NONE) return fr * rinv2;
   const float kr = p.kappa * r;
   const float a = kind == 0 ? erfcf(kr) : (kind == 1 ? p.e14fac - erff(kr) : -erff(kr));
   const float e = qq * a * rinv;
@@ -101,6 +103,8 @@ __device__ __forceinline__ double pair_terms_f64(double r2, double qq, double c6
     u_vdw = c12 * (1.0 / 12.0) * (rinv12 + 2.0 * r6 * p.ro18d - 3.0 * p.ro12d) -
             c6 * (1.0 / 6.0) * (rinv6 + r6 * p.ro12d - 2.0 * p.ro6d);
   }
+  u_elec = 0.0;
+  if (p.elec == PME_ELEC_NONE) return fr * rinv2;
   if (p.tab != nullptr && r2 >= p.tab_s0) {
     const double u = (r2 - p.tab_s0) * p.tab_invh;
     const int i = min((int)u, p.tab_n - 1);

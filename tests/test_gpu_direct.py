@@ -201,3 +201,27 @@ def test_direct_dense_cells_many_chunks(cuda, oracle, box, n):
     assert abs(e["elec"] - ee) <= 1e-7 * abs(ee) + 1e-6
     assert np.abs(vir - vo).max() <= 1e-6 * np.abs(vo).max()
     dr.close()
+
+
+def test_direct_vdw_only(cuda, oracle):
+    """ELEC_NONE: only the shifted Lennard-Jones terms (the oracle with the charges set to 0)."""
+    from gpu_recip_b200.direct import CudaPMEDirectForce, ELEC_NONE, VDW_VSH
+    d = _lattice()
+    n = d["xyzq"].shape[0]
+    dr = CudaPMEDirectForce()
+    dr.setup(24.0, 24.0, 24.0, 0.35, 9.0, 7.5, 1.0, VDW_VSH, ELEC_NONE)
+    dr.set_vdwparam(d["vdwparam"])
+    dr.set_vdwtype(d["vdwtype"])
+    dr.set_exclusions(d["iblo14"], d["inb14"])
+    x = cuda.from_numpy(d["xyzq"]).cuda()
+    fi, e, vir = _run(cuda, dr, x, n, n)
+    xq0 = d["xyzq"].astype(np.float64).copy()
+    xq0[:, 3] = 0.0
+    ptr, idx = oracle.exclusions_csr(d["iblo14"], d["inb14"], n)
+    fo, ev, ee, vo = oracle.direct_force(xq0, d["box"], 0.35, 9.0, d["vdwparam"].astype(np.float32).astype(np.float64),
+                                         d["vdwtype"], ptr, idx)
+    f = fi.astype(np.float64) / FORCE_SCALE
+    assert e["elec"] == 0.0 and ee == 0.0
+    assert np.sqrt(((f - fo) ** 2).sum() / (fo ** 2).sum()) <= 1e-6
+    assert abs(e["vdw"] - ev) <= 1e-6 * abs(ev)
+    dr.close()
