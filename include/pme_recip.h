@@ -278,8 +278,9 @@ PME_API int pme_server_get_stats(pme_server* s, pme_server_stats* out);
  * locks.  Same spreading kernel and exact int64 fixed-point accumulation as pme_spread_charge,
  * but the accumulation grid is a fixed array compiled into this library (8 MiB on every GPU that
  * loads it, so nfftx*nffty*nfftz <= 1048576; larger grids return PME_EINVAL).  The caller passes
- * the coordinates (device float4[ncoord]), the host recip[9] and the output: grid_out, a device
- * float[nfftz][nffty][nfftx] that receives the converted charge grid.  Asynchronous on `stream`.
+ * the coordinates (device float4[ncoord]), the host recip[9] (orthorhombic: a positive diagonal,
+ * off-diagonals return PME_EINVAL) and the output: grid_out, a device float[nfftz][nffty][nfftx]
+ * that receives the converted charge grid.  Asynchronous on `stream`.
  * The first call on a device looks up the array's device address (cudaGetSymbolAddress): make it
  * before any stream capture.  All calls share the array and each clears it before use: calls
  * whose work overlaps on the GPU race and corrupt each other's grid. */
