@@ -52,6 +52,7 @@ SIGNATURES = {
     "pme_set_energy_virial_mirror": [_P, _P],
     "pme_eval_ortho": [_P, _D, _D, _D, _P, _I, _D, _I, _I, _I, _P, _I],
     "pme_eval": [_P, _DP, _P, _I, _D, _I, _I, _I, _P, _I],
+    "pme_eval_host": [_P, _DP, _P, _I, _D, _I, _I, _I, _P, _I],
     "pme_copy_charge_grid_fixed": [_P, _P],
     "pme_copy_charge_grid": [_P, _P],
     "pme_copy_fft_grid": [_P, _P],

@@ -63,6 +63,8 @@ struct SysDesc {
   double* ev_mirror;         // optional device-mapped host copy of each evaluation's own record
   int tx_rows, tx_y, tx_z;   // lines per tile of the x, y, z passes
   int plane;                 // 1: the fused path runs y, z and the solve as whole-plane tiles
+  int bin_atoms;             // atoms per bin tile of the fused path (0: kThreads)
+  int xyzq_host;             // 1: xyzq is pinned host memory, read once in index order
   // Atom bins of the fused path: bin (by, bz) holds the atoms whose stencil origin (iy0, iz0)
   // lies in row block [by*bry, by*bry+bry) x [bz*brz, bz*brz+brz); fixed capacity bin_cap per bin,
   // surplus atoms go to an overflow list.  Counters are double-buffered by launch parity.
@@ -96,7 +98,9 @@ __host__ __device__ inline int tiles_xpass(const SysDesc& d) { return (d.g.ny * 
 __host__ __device__ inline int tiles_ypass(const SysDesc& d) { return (d.g.hx * d.g.nz + d.tx_y - 1) / d.tx_y; }
 __host__ __device__ inline int tiles_zpass(const SysDesc& d) { return ((d.g.ny + d.tx_z - 1) / d.tx_z) * d.g.hx; }
 __host__ __device__ inline int tiles_plane(const SysDesc& d) { return d.g.hx; }
-__host__ __device__ inline int tiles_bin(const SysDesc& d) { return (d.natom + kThreads - 1) / kThreads; }
+// atoms per bin tile: kThreads, or fewer when the host asks for more, smaller tiles (bin_atoms)
+__host__ __device__ inline int bin_tile_atoms(const SysDesc& d) { return d.bin_atoms > 0 ? d.bin_atoms : kThreads; }
+__host__ __device__ inline int tiles_bin(const SysDesc& d) { return (d.natom + bin_tile_atoms(d) - 1) / bin_tile_atoms(d); }
 __host__ __device__ inline int tiles_blocks(const SysDesc& d) { return d.nby * d.nbz; }
 // Lanes per atom of the gather (staged and fused): as few as keep the rows of one lane,
 // P^2 / lanes, at 8-9, so that a bin's atoms take few passes.
@@ -674,11 +678,12 @@ __device__ __forceinline__ void bin_tile_p(const SysDesc& d, int tile, int parit
   constexpr int NW = RF - 8;                   // weight floats incl. padding
   const Geom& g = d.g;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int idx = tile * kThreads + threadIdx.x;
-  const bool valid = idx < d.natom;
+  const int idx = tile * bin_tile_atoms(d) + threadIdx.x;
+  const bool valid = (int)threadIdx.x < bin_tile_atoms(d) && idx < d.natom;
   const int nbins = d.nby * d.nbz;
-  // walk the atoms in the previous evaluation's bin-sorted order when it is one for this count
-  const bool sorted = __ldcg(&d.bin_meta[kMetaPermNatom]) == d.natom;
+  // walk the atoms in the previous evaluation's bin-sorted order when it is one for this count;
+  // coordinates in host memory are read in index order (whole lines over the bus, not 16 bytes)
+  const bool sorted = !d.xyzq_host && __ldcg(&d.bin_meta[kMetaPermNatom]) == d.natom;
   const int i = valid && sorted ? __ldcg(&d.perm[idx]) : idx;
   step_mark(d, 16);
   long long q2 = 0;

@@ -235,6 +235,22 @@ class CudaPMERecip:
                                    float(kappa), int(calc_energy), int(calc_virial), k, _ptr(force),
                                    int(stride)), "eval")
 
+    def eval_host(self, recip, xyzq, ncoord: int, kappa: float, calc_energy: bool, calc_virial: bool,
+                  force, stride: int = 0, kind: Optional[int] = None):
+        """pme_eval from and to page-locked host tensors (``tensor.pin_memory()``): the evaluation
+        reads the coordinates over the bus itself and the forces come back by one copy on the
+        stream; they are in ``force`` once the stream has passed the call."""
+        import torch
+        for t, what in ((xyzq, "xyzq"), (force, "force")):
+            if not isinstance(t, torch.Tensor) or t.is_cuda or not t.is_pinned() or not t.is_contiguous():
+                raise ValueError(f"{what} must be a contiguous pinned host tensor")
+        if xyzq.dtype != torch.float32 or xyzq.numel() < 4 * ncoord:
+            raise ValueError("xyzq must be float32 (x, y, z, q) for ncoord atoms")
+        k = self._force_kind(force, stride) if kind is None else kind
+        C.check(self._lib.pme_eval_host(self._h, C.dbl9(recip), ctypes.c_void_p(xyzq.data_ptr()), ncoord,
+                                        float(kappa), int(calc_energy), int(calc_virial), k,
+                                        ctypes.c_void_p(force.data_ptr()), int(stride)), "eval_host")
+
     def eval_ortho(self, inv_box, xyzq, ncoord: int, kappa: float, calc_energy: bool,
                    calc_virial: bool, force, stride: int = 0, kind: Optional[int] = None):
         k = self._force_kind(force, stride) if kind is None else kind

@@ -114,6 +114,17 @@ PME_API int pme_eval_ortho(pme_recip* h, double inv_boxx, double inv_boxy, doubl
  * orthorhombic boxes (CudaDomdecRecip.h:20-23 builds a diagonal recip). */
 PME_API int pme_eval(pme_recip* h, const double* recip, const void* xyzq, int ncoord, double kappa,
                    int calc_energy, int calc_virial, int kind, void* force, int stride);
+/* pme_eval from and to host buffers: xyzq_host is page-locked host memory mapped at the same
+ * address (cudaHostAlloc / cudaMallocHost with unified addressing), which the evaluation reads
+ * directly over the bus, in index order, while it bins the atoms; force_host is page-locked host
+ * memory that receives the forces by one copy on the handle's stream after the evaluation (for
+ * PME_FORCE_F32_SOA only the ncoord entries of each of the three rows).  Float kinds only
+ * (PME_EUNSUPPORTED for PME_FORCE_I64_SOA_ACCUM); PME_EINVAL for memory that is not page-locked.
+ * Asynchronous: the forces are in force_host once the stream has passed the call.  Same results
+ * as pme_eval bit for bit.  No counterpart in the reference, whose calls take device buffers. */
+PME_API int pme_eval_host(pme_recip* h, const double* recip, const void* xyzq_host, int ncoord,
+                          double kappa, int calc_energy, int calc_virial, int kind, void* force_host,
+                          int stride);
 
 /* ---- grid read-back for parity checks (synchronise the stream; host outputs) ----
  * Layouts follow the reference: real grids [z][y][x]; half-complex grid [z][y][kx],
