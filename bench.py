@@ -60,6 +60,8 @@ def parse():
                     help="timed evaluations of the 24,000-atom rhombic dodecahedron (0: skip)")
     ap.add_argument("--direct-steps", type=int, default=200,
                     help="timed direct-space evaluations of the reference's 23,558-atom system (0: skip)")
+    ap.add_argument("--reference-gpu-steps", type=int, default=200,
+                    help="timed evaluations of the reference's own CUDA operator on this GPU (0: skip)")
     ap.add_argument("--serve-requests", type=int, default=600, help="requests of the serving run (0: skip)")
     ap.add_argument("--serve-rate", type=float, default=400.0, help="Poisson arrival rate (requests/s)")
     return ap.parse_args()
@@ -371,6 +373,11 @@ def run_b200(args):
     if args.serve_requests > 0:
         serving = run_serving(args, dev, rank, world)
 
+    # ---- the reference's own CUDA operator on this GPU (timing comparator, single GPU only) --------
+    reference_gpu = None
+    if rank == 0 and world == 1 and args.reference_gpu_steps > 0:
+        reference_gpu = run_reference_gpu(s, args, float(np.percentile(per, 50)) * 1000.0, float(ev_step[0].item()))
+
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         rate, cnt, dt, cores = cpu_oracle_rate(s, args.cpu_seconds)
@@ -393,7 +400,7 @@ def run_b200(args):
                 "gpu_launches": kernels_per_eval * K,
                 "roofline": roofline, "batched": batched, "serving": serving, "large": large,
                 "triclinic": triclinic, "direct": direct,
-                "fft_comparator": fft_cmp,
+                "fft_comparator": fft_cmp, "reference_gpu": reference_gpu,
                 "clocks": clocks.summary(), "cpu_baseline": cpu}
         print(json.dumps(line), flush=True)
     R.barrier()
@@ -509,6 +516,43 @@ def run_large(args, dev, stream, flush, rank, world):
             "roofline_frac": s.alg_bytes() / (ms * 1e-3) / 1e9 / peak,
             "launch_shape": {k: tune[k] for k in ("schedule", "x_lines", "y_lines", "z_columns", "grid_ctas")},
             "staged_stages": per_stage}
+
+
+REF_GPU_BIN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "baseline", "_ref", "ref_gpu_bench")
+
+
+def run_reference_gpu(s, args, b200_us_p50: float, b200_energy: float):
+    """Times the reference's own operator, CudaPMERecip<float, float, float2> built from its
+    unmodified sources (baseline/ref_gpu), on this GPU and workload: per evaluation the sequence of
+    its test driver (record clear, spread, R2C, solve with energy and virial, C2R, gather, self
+    energy) with L2 flushed in between, BOX (3-D cuFFT) and COLUMN (1-D cuFFTs and transposes)
+    modes.  It runs as a child process: the reference exits the process on a CUDA error.  Timing
+    only: with CUDA 12.9's cuFFT its in-place transforms no longer get the unpadded layout they
+    were written for, so its results are not valid (reported as result_valid)."""
+    import struct
+    import subprocess
+    if not os.path.exists(REF_GPU_BIN):
+        return {"unavailable": "baseline/_ref/ref_gpu_bench not built (needs the reference's sources at build time)"}
+    out = {"operator": "reference CudaPMERecip<float, float, float2> (gpu_recip), unmodified sources, "
+                       "compiled for sm_100a with compatibility shims", "l2": "flushed (256 MiB memset) before every evaluation"}
+    for ft, name in ((2, "box"), (0, "column")):
+        hdr = struct.pack("<9i4x4d", s.natom, *s.nfft, s.order, ft, 3, args.reference_gpu_steps, 0, s.kappa, *s.box)
+        try:
+            p = subprocess.run([REF_GPU_BIN], input=hdr + np.ascontiguousarray(s.xyzq, dtype=np.float32).tobytes(),
+                               capture_output=True, timeout=300)
+        except subprocess.TimeoutExpired:
+            out[name] = {"unavailable": "timed out"}
+            continue
+        if p.returncode != 0:
+            out[name] = {"unavailable": f"exit {p.returncode}: {p.stderr.decode(errors='replace')[-300:]}"}
+            continue
+        r = json.loads(p.stdout.decode().strip().splitlines()[-1])
+        e = r["energy_recip"]
+        valid = e is not None and abs(e - b200_energy) <= 1e-4 * abs(b200_energy)
+        out[name] = {"us_per_eval_p50": r["us_p50"], "us_per_eval_mean": r["us_mean"], "steps": r["steps"],
+                     "evals_per_s": 1e6 / r["us_mean"], "energy_recip": e, "result_valid": bool(valid),
+                     "b200_speedup_p50": r["us_p50"] / b200_us_p50}
+    return out
 
 
 def run_triclinic(args, dev, stream, flush, rank, world):
