@@ -38,7 +38,7 @@ METRIC = "PME recip evals/s at 24k atoms/64^3; batched evals/s + p50/p99 latency
 
 # DRAM bytes (read + write) of one k_fused launch from an ncu capture, by workload (mean of 3
 # launches; profiles/k_fused_water8k_64_p4_full.md).  None where not captured.
-TRAFFIC_BYTES = {"water8k_64_p4": 659968}
+TRAFFIC_BYTES = {"water8k_64_p4": 660139}
 UNIT = "evals/s"
 FALLBACK_HBM_GBS = 6650.0
 

@@ -63,6 +63,7 @@ SIGNATURES = {
     "pme_reserve_atoms": [_P, _I],
     "pme_set_fault_injection": [_P, _I],
     "pme_set_fft_schedule": [_P, _I],
+    "pme_set_x_gather_fusion": [_P, _I],
     "pme_batch_create": [_P, _I, _P, ctypes.POINTER(_P)],
     "pme_batch_destroy": [_P],
     "pme_batch_set_stream": [_P, _P],
@@ -110,6 +111,7 @@ _RESTYPES = {"pme_last_error_string": ctypes.c_char_p, "pme_status_string": ctyp
 
 PME_INJECT_NONE, PME_INJECT_SKIP_BARRIER = 0, 1
 PME_SCHED_AUTO, PME_SCHED_PLANES, PME_SCHED_PASSES = 0, 1, 2
+PME_XGATHER_AUTO, PME_XGATHER_OFF = 0, 1
 
 
 class SystemDesc(ctypes.Structure):

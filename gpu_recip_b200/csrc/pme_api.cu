@@ -54,6 +54,7 @@ struct pme_recip {
   double* ev_mirror = nullptr;   // device-mapped pinned host memory, or null
   int plane_mode = 0;   // 0 automatic, 1 whole-plane tiles where they fit, 2 separate passes
   int grid_cap = 0;     // CTAs of the persistent launch (0: as many as are resident)
+  int x_gather = PME_XGATHER_AUTO;   // PME_XGATHER_*
   float* d_force = nullptr;      // pme_eval_host: device forces before the copy to the host
   size_t force_bytes = 0;
 };
@@ -141,6 +142,10 @@ int launch_fused_single(pme_recip* h, const SysDesc& d_in) {
   // where the hardware doubles CTAs up (measured on 24,000 atoms: 0.9 us faster; 64-atom tiles
   // were 2 us slower)
   d.bin_atoms = (d.natom + kThreads - 1) / kThreads < sms ? kThreads / 2 : kThreads;
+  // inverse x pass inside the gather tiles where its rows fit in the shared memory the other
+  // phases already take (so that the launch keeps its CTAs per SM)
+  d.gx = 0;
+  if (h->x_gather == PME_XGATHER_AUTO && gx_smem_bytes(d.g.nx, d.bry, d.brz, d.order) <= fused_smem_bytes(d)) d.gx = 1;
   fused_tile_counts(d, a.total);
   a.nbar = fused_barriers(a.total);
   a.single = d;
@@ -610,6 +615,13 @@ int pme_set_fft_schedule(pme_recip* h, int schedule) {
   if (int rc = handle_ok(h)) return rc;
   if (schedule < PME_SCHED_AUTO || schedule > PME_SCHED_PASSES) return fail(PME_EINVAL, "unknown schedule");
   h->plane_mode = schedule;
+  return PME_OK;
+}
+
+int pme_set_x_gather_fusion(pme_recip* h, int mode) {
+  if (int rc = handle_ok(h)) return rc;
+  if (mode != PME_XGATHER_AUTO && mode != PME_XGATHER_OFF) return fail(PME_EINVAL, "unknown x-gather fusion mode");
+  h->x_gather = mode;
   return PME_OK;
 }
 

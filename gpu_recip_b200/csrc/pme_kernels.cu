@@ -242,7 +242,14 @@ __device__ __forceinline__ void fused_body(const FusedArgs& a) {
           if (local < tiles_xpass(d)) x_inv_tile(d, local, smem);
           else if (threadIdx.x == 0) finalize_system(d, true, true);
           break;
-        default: gather_bin_dispatch(d, local, parity, (char*)smem); break;
+        default:
+          // with the inverse x pass in the gather tiles, the record is finalised by one extra tile here
+          if (d.gx && local == tiles_blocks(d)) {
+            if (threadIdx.x == 0) finalize_system(d, true, true);
+          } else {
+            gather_bin_dispatch(d, local, parity, (char*)smem);
+          }
+          break;
       }
       __syncthreads();
     }
@@ -283,6 +290,10 @@ size_t fused_smem_bytes(const SysDesc& d) {
                  staged_z_smem(d), d.plane ? plane_smem_bytes(d.g.ny, d.g.nz) : 0,
                  spread_x_smem_bytes(d.g.nx, d.bry * d.brz, d.order)};
   for (size_t v : c) m = m > v ? m : v;
+  if (d.gx) {
+    const size_t v = gx_smem_bytes(d.g.nx, d.bry, d.brz, d.order);
+    m = m > v ? m : v;
+  }
   return m;
 }
 
@@ -292,8 +303,8 @@ void fused_tile_counts(const SysDesc& d, int* counts) {
   counts[2] = d.plane ? tiles_plane(d) : tiles_ypass(d);
   counts[3] = d.plane ? 0 : tiles_zpass(d);
   counts[4] = d.plane ? 0 : tiles_ypass(d);
-  counts[5] = tiles_xpass(d) + 1;
-  counts[6] = tiles_blocks(d);
+  counts[5] = d.gx ? 0 : tiles_xpass(d) + 1;
+  counts[6] = tiles_blocks(d) + (d.gx ? 1 : 0);
 }
 
 int fused_barriers(const int* total) {

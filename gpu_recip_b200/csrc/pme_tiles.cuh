@@ -65,6 +65,8 @@ struct SysDesc {
   int plane;                 // 1: the fused path runs y, z and the solve as whole-plane tiles
   int bin_atoms;             // atoms per bin tile of the fused path (0: kThreads)
   int xyzq_host;             // 1: xyzq is pinned host memory, read once in index order
+  int gx;                    // 1: each gather tile runs the inverse x pass of the rows it reads
+                             // (fused path; no x-inverse phase)
   // Atom bins of the fused path: bin (by, bz) holds the atoms whose stencil origin (iy0, iz0)
   // lies in row block [by*bry, by*bry+bry) x [bz*brz, bz*brz+brz); fixed capacity bin_cap per bin,
   // surplus atoms go to an overflow list.  Counters are double-buffered by launch parity.
@@ -1195,10 +1197,18 @@ struct GatherSplines {
   int xs[P];
 };
 
+// Where a gather reads the solved real grid: the global rgrid, or (GX) a window of rows in shared
+// memory: row t = j + ry i holds grid row (y0 + j, z0 + i) wrapped, x fastest; every atom of the
+// window's tile has its stencil origin in [y0, y0 + bry) x [z0, z0 + brz).
+struct RowWin {
+  const float* rows;
+  int y0, z0, ry;
+};
+
 // Sum of the rows r = g, g+8, g+16, ... < P^2 (group g) for the three force components.
-template <int P>
+template <int P, bool GX = false>
 __device__ __forceinline__ float3 gather_group(const SysDesc& d, const GatherSplines<P>& sp, int g, int iy, int iz,
-                                               bool valid) {
+                                               bool valid, const RowWin& w) {
   const Geom& gm = d.g;
   constexpr int RPG = (P * P + 7) / 8;
   float f1 = 0.0f, f2 = 0.0f, f3 = 0.0f;
@@ -1213,8 +1223,13 @@ __device__ __forceinline__ float3 gather_group(const SysDesc& d, const GatherSpl
         if (q == b) { wy = sp.thy[q]; dwy = sp.dthy[q]; }
         if (q == c) { wz = sp.thz[q]; dwz = sp.dthz[q]; }
       }
-      const int y = wrap_add(iy, b, gm.ny), z = wrap_add(iz, c, gm.nz);
-      const float* row = d.rgrid + (size_t)gm.nx * (y + (size_t)gm.ny * z);
+      const float* row;
+      if (GX) {
+        row = w.rows + (size_t)gm.nx * ((iy - w.y0 + b) + w.ry * (iz - w.z0 + c));
+      } else {
+        const int y = wrap_add(iy, b, gm.ny), z = wrap_add(iz, c, gm.nz);
+        row = d.rgrid + (size_t)gm.nx * (y + (size_t)gm.ny * z);
+      }
       float s1 = 0.0f, s2 = 0.0f;
 #pragma unroll
       for (int i = 0; i < P; i++) {
@@ -1232,9 +1247,10 @@ __device__ __forceinline__ float3 gather_group(const SysDesc& d, const GatherSpl
 
 __device__ __forceinline__ float3 add3(float3 a, float3 b) { return make_float3(a.x + b.x, a.y + b.y, a.z + b.z); }
 
-template <int P, int KIND, int LPA>
+template <int P, int KIND, int LPA, bool GX = false>
 __device__ __forceinline__ void gather_core(const SysDesc& d, int atom, bool valid, int gl, int ix, int iy, int iz,
-                                            float ux, float uy, float uz, float q) {
+                                            float ux, float uy, float uz, float q,
+                                            const RowWin& w = RowWin{nullptr, 0, 0, 0}) {
   static_assert(LPA == 2 || LPA == 4 || LPA == 8, "lanes per atom");
   const Geom& g = d.g;
   GatherSplines<P> sp;
@@ -1246,12 +1262,14 @@ __device__ __forceinline__ void gather_core(const SysDesc& d, int atom, bool val
   // this lane's groups gl + LPA m, combined locally in the tree's order
   float3 f;
   if (LPA == 8) {
-    f = gather_group<P>(d, sp, gl, iy, iz, valid);
+    f = gather_group<P, GX>(d, sp, gl, iy, iz, valid, w);
   } else if (LPA == 4) {
-    f = add3(gather_group<P>(d, sp, gl, iy, iz, valid), gather_group<P>(d, sp, gl + 4, iy, iz, valid));
+    f = add3(gather_group<P, GX>(d, sp, gl, iy, iz, valid, w), gather_group<P, GX>(d, sp, gl + 4, iy, iz, valid, w));
   } else {
-    const float3 a = add3(gather_group<P>(d, sp, gl, iy, iz, valid), gather_group<P>(d, sp, gl + 4, iy, iz, valid));
-    const float3 b = add3(gather_group<P>(d, sp, gl + 2, iy, iz, valid), gather_group<P>(d, sp, gl + 6, iy, iz, valid));
+    const float3 a = add3(gather_group<P, GX>(d, sp, gl, iy, iz, valid, w),
+                          gather_group<P, GX>(d, sp, gl + 4, iy, iz, valid, w));
+    const float3 b = add3(gather_group<P, GX>(d, sp, gl + 2, iy, iz, valid, w),
+                          gather_group<P, GX>(d, sp, gl + 6, iy, iz, valid, w));
     f = add3(a, b);
   }
 #pragma unroll
@@ -1317,11 +1335,66 @@ __device__ __forceinline__ void gather_tile(const SysDesc& d, int tile) {
 // gathered.  The tile also writes its atoms into the system's bin-sorted atom order at the bin's
 // offset; the next evaluation's binning walks the atoms in that order, so that the atoms of a warp
 // share a few bins.  Overflow atoms follow all binned ones.
-template <int P, int KIND, int LPA>
-__device__ __forceinline__ void gather_bin_tile(const SysDesc& d, int tile, int parity, int* red) {
+// Shared memory of a gather tile that runs its own inverse x pass: 64 bytes of reduction space,
+// the x twiddles, and two FFT buffers of nx lines x (rows + 1, odd) for the (bry + P - 1) x
+// (brz + P - 1) rows its atoms reach.
+__host__ __device__ inline int gx_rows_count(int bry, int brz, int order) { return (bry + order - 1) * (brz + order - 1); }
+__host__ __device__ inline int gx_ld(int rows) { return (rows + 1) | 1; }
+__host__ __device__ inline size_t gx_smem_bytes(int nx, int bry, int brz, int order) {
+  const int R = gx_rows_count(bry, brz, order);
+  return 64 + (size_t)nx * 8 + 2 * (size_t)nx * gx_ld(R) * 8;
+}
+
+// The inverse x pass of the rows a gather tile reads (bin (y0 / bry, z0 / brz)): Hermitian
+// rebuild, inverse FFT and real part of each row, the same lines with the same arithmetic as
+// x_inv_tile (so the same bits), into real rows in shared memory (RowWin layout).  The rows of
+// the halo are transformed again by the neighbouring bins' tiles: about (1 + (P-1)/bry)^2 times
+// the x-inverse work, for one grid barrier and one pass over the real grid less.
+template <int P>
+__device__ __forceinline__ RowWin gx_rows(const SysDesc& d, int y0, int z0, char* smem_raw) {
+  const Geom& g = d.g;
+  const FftPlan1D& plan = d.px;
+  const int L = g.nx, hx = g.hx, RY = d.bry + P - 1, R = gx_rows_count(d.bry, d.brz, P), ld = gx_ld(R);
+  float2* tw = (float2*)(smem_raw + 64);
+  float2* b0 = tw + L;
+  float2* b1 = b0 + (size_t)L * ld;
+  const int tid = threadIdx.x;
+  for (int i = tid; i < L; i += kThreads) tw[i] = __ldg(&d.tw[plan.tw_off + i]);
+  const FastDiv Rd = make_fastdiv(R), RYd = make_fastdiv(RY);
+  for (int idx = tid; idx < hx * R; idx += kThreads) {
+    const int k = fdiv(idx, Rd), t = idx - k * R;
+    const int i = fdiv(t, RYd), j = t - i * RY;
+    const int y = (y0 + j) % g.ny, z = (z0 + i) % g.nz;
+    const float2 v = __ldcg(&d.cgrid[cidx(g, k, z, y)]);
+    b0[k * ld + t] = v;
+    if (k >= 1 && L - k >= hx) b0[(L - k) * ld + t] = make_float2(v.x, -v.y);
+  }
+  __syncthreads();
+  TileLane ln(tid, kThreads, R);
+  float2* res = fft_tile(b0, b1, plan, ld, 1, ln, tw, true);
+  float* rows = (float*)(res == b0 ? b1 : b0);
+  // the tile's own rows (its bin's row block) also go to the global solved grid, which therefore
+  // holds the whole grid after the evaluation, as after the separate x-inverse phase
+  const int ymax = min(d.bry, g.ny - y0), zmax = min(d.brz, g.nz - z0);
+  for (int idx = tid; idx < L * R; idx += kThreads) {
+    const int t = fdiv(idx, plan.n_div), e = idx - t * L;
+    const float v = res[e * ld + t].x;
+    rows[t * L + e] = v;
+    const int i = fdiv(t, RYd), j = t - i * RY;
+    if (j < ymax && i < zmax) __stcg(&d.rgrid[((size_t)(z0 + i) * g.ny + (y0 + j)) * L + e], v);
+  }
+  __syncthreads();
+  return RowWin{rows, y0, z0, RY};
+}
+
+template <int P, int KIND, int LPA, bool GX = false>
+__device__ __forceinline__ void gather_bin_tile(const SysDesc& d, int tile, int parity, char* smem_raw) {
   constexpr int RF = rec_floats(P);
   const int nbins = d.nby * d.nbz;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  int* red = (int*)smem_raw;
+  RowWin w{nullptr, 0, 0, 0};
+  if (GX) w = gx_rows<P>(d, (tile % d.nby) * d.bry, (tile / d.nby) * d.brz, smem_raw);
   const int* counts = d.bin_count + parity * nbins;
   const int cnt = min(__ldcg(&counts[tile]), d.bin_cap);
   const float* list = d.bin_recs + (size_t)tile * d.bin_cap * RF;
@@ -1368,8 +1441,8 @@ __device__ __forceinline__ void gather_bin_tile(const SysDesc& d, int tile, int 
     const int atom = __float_as_int(h.w);
     // warps whose atoms all lie beyond the bin's count skip the pass (the test is warp-uniform)
     if (j0 + (warp * 32) / LPA < cnt)
-      gather_core<P, KIND, LPA>(d, atom, valid, gl, __float_as_int(h.x), __float_as_int(h.y), __float_as_int(h.z), u.x,
-                           u.y, u.z, u.w);
+      gather_core<P, KIND, LPA, GX>(d, atom, valid, gl, __float_as_int(h.x), __float_as_int(h.y), __float_as_int(h.z),
+                                    u.x, u.y, u.z, u.w, w);
     if (valid && gl == 0) d.perm[pre + j] = atom;
     h = hn;
     u = un;
@@ -1388,8 +1461,8 @@ __device__ __forceinline__ void gather_bin_tile(const SysDesc& d, int tile, int 
       if (tile == 0 && gl == 0) d.perm[tot + j] = __float_as_int(hh.w);
     }
     if (j0 + (warp * 32) / LPA < novf)
-      gather_core<P, KIND, LPA>(d, __float_as_int(hh.w), mine, gl, __float_as_int(hh.x), __float_as_int(hh.y),
-                           __float_as_int(hh.z), uu.x, uu.y, uu.z, uu.w);
+      gather_core<P, KIND, LPA, GX>(d, __float_as_int(hh.w), mine, gl, __float_as_int(hh.x), __float_as_int(hh.y),
+                                    __float_as_int(hh.z), uu.x, uu.y, uu.z, uu.w, w);
   }
   // binned + overflow atoms are all natom atoms: the order is a permutation for this atom count
   if (tile == 0 && tid == 0) d.bin_meta[kMetaPermNatom] = d.natom;
@@ -1412,21 +1485,27 @@ __device__ __forceinline__ void gather_dispatch(const SysDesc& d, int tile) {
   }
 }
 
-template <int P>
-__device__ __forceinline__ void gather_bin_any(const SysDesc& d, int tile, int parity, int* red) {
+template <int P, bool GX>
+__device__ __forceinline__ void gather_bin_any(const SysDesc& d, int tile, int parity, char* smem) {
   switch (d.force_kind) {
-    case kForceF32Soa: gather_bin_tile<P, kForceF32Soa, gather_lanes(P)>(d, tile, parity, red); break;
-    case kForceF32x3: gather_bin_tile<P, kForceF32x3, gather_lanes(P)>(d, tile, parity, red); break;
-    default: gather_bin_tile<P, kForceI64SoaAccum, gather_lanes(P)>(d, tile, parity, red); break;
+    case kForceF32Soa: gather_bin_tile<P, kForceF32Soa, gather_lanes(P), GX>(d, tile, parity, smem); break;
+    case kForceF32x3: gather_bin_tile<P, kForceF32x3, gather_lanes(P), GX>(d, tile, parity, smem); break;
+    default: gather_bin_tile<P, kForceI64SoaAccum, gather_lanes(P), GX>(d, tile, parity, smem); break;
+  }
+}
+
+template <bool GX>
+__device__ __forceinline__ void gather_bin_order(const SysDesc& d, int tile, int parity, char* smem) {
+  switch (d.order) {
+    case 4: gather_bin_any<4, GX>(d, tile, parity, smem); break;
+    case 6: gather_bin_any<6, GX>(d, tile, parity, smem); break;
+    default: gather_bin_any<8, GX>(d, tile, parity, smem); break;
   }
 }
 
 __device__ __forceinline__ void gather_bin_dispatch(const SysDesc& d, int tile, int parity, char* smem) {
-  switch (d.order) {
-    case 4: gather_bin_any<4>(d, tile, parity, (int*)smem); break;
-    case 6: gather_bin_any<6>(d, tile, parity, (int*)smem); break;
-    default: gather_bin_any<8>(d, tile, parity, (int*)smem); break;
-  }
+  if (d.gx) gather_bin_order<true>(d, tile, parity, smem);
+  else gather_bin_order<false>(d, tile, parity, smem);
 }
 
 __device__ __forceinline__ void spread_dispatch(const SysDesc& d, int tile, void* smem) {

@@ -313,6 +313,10 @@ class CudaPMERecip:
         """PME_SCHED_AUTO / PME_SCHED_PLANES / PME_SCHED_PASSES (identical results)."""
         C.check(self._lib.pme_set_fft_schedule(self._h, int(schedule)), "set_fft_schedule")
 
+    def set_x_gather_fusion(self, mode: int):
+        """PME_XGATHER_AUTO (default) / PME_XGATHER_OFF (identical results)."""
+        C.check(self._lib.pme_set_x_gather_fusion(self._h, int(mode)), "set_x_gather_fusion")
+
     def autotune(self, inv_box, xyzq, ncoord: int, kappa: float, reps: int = 10) -> dict:
         """Measure launch shapes of the fused evaluation on this system and keep the fastest
         (pme_autotune); returns the chosen shape and its time per evaluation."""

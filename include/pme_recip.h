@@ -182,6 +182,14 @@ PME_API int pme_set_tune_config(pme_recip* h, const pme_tune_config* cfg);
 PME_API int pme_tune_cache_clear(void);
 PME_API int pme_set_fft_schedule(pme_recip* h, int schedule);
 
+/* Where the fused evaluation runs the inverse x pass.  AUTO (default): inside the gather tiles,
+ * each transforming the rows its atoms reach (halo rows again for every tile that reaches them),
+ * when those rows fit in the shared memory the other phases take (each tile also stores its own
+ * rows, so the solved grid is complete afterwards, as the staged calls expect).  OFF: as a phase
+ * of its own before the gather.  Results are identical bit for bit; only the time differs. */
+enum { PME_XGATHER_AUTO = 0, PME_XGATHER_OFF = 1 };
+PME_API int pme_set_x_gather_fusion(pme_recip* h, int mode);
+
 /* Test hook for failure detection: PME_INJECT_SKIP_BARRIER makes CTA 0 of the next fused
  * evaluations leave before the first grid barrier, so the other CTAs' bounded waits run out
  * (no fault, no hang).  PME_INJECT_NONE turns it off. */

@@ -94,3 +94,50 @@ def test_batch_autotune_keeps_results(cuda):
     assert np.array_equal(ev0, ev1)
     for a, f in zip(f0, forces):
         assert np.array_equal(a, f.cpu().numpy())
+
+
+@pytest.mark.parametrize("system", ["water8k_64_p4", "water8k_64_p6", "water1k_32", "dodec_64_p4", "odd_p4"])
+def test_inverse_x_in_the_gather_gives_the_same_bits(cuda, system):
+    """The fused evaluation with the inverse x pass inside the gather tiles (each tile transforms
+    the rows its atoms reach) equals the one with a separate x-inverse phase bit for bit: forces of
+    every kind, energy, virial and the stored solved grid; repeated evaluations too."""
+    torch = cuda
+    from gpu_recip_b200 import CudaPMERecip, force_stride, _capi as C
+    s = {"water8k_64_p4": lambda: S.config_production(4), "water8k_64_p6": lambda: S.config_production(6),
+         "water1k_32": S.config_small, "dodec_64_p4": lambda: S.config_triclinic(4),
+         "odd_p4": lambda: S.PmeSystem("odd", S.config_small().xyzq, S.config_small().box, (30, 36, 25), 4, 0.34)}[system]()
+    n = s.natom
+    st = force_stride(n)
+    x = torch.from_numpy(s.xyzq).cuda()
+
+    def run(mode):
+        pme = CudaPMERecip(*s.nfft, s.order)
+        pme.set_x_gather_fusion(mode)
+        outs = []
+        for rep in range(2):
+            f = torch.zeros(3 * st, dtype=torch.float32, device="cuda")
+            fi = torch.full((3 * st,), 5, dtype=torch.int64, device="cuda")
+            pme.energy_virial.clear()
+            pme.eval(s.recip9, x, n, s.kappa, True, True, f, st)
+            pme.eval(s.recip9, x, n, s.kappa, False, False, fi, st)
+            torch.cuda.synchronize()
+            pme.energy_virial.copyToHost()
+            outs.append((f.cpu().numpy(), fi.cpu().numpy(), pme.energy_virial.getEnergy("recip"),
+                         pme.energy_virial.getEnergy("self"), pme.energy_virial.getVirial(),
+                         pme.solved_grid()))   # the whole solved grid is stored either way
+        return outs
+
+    fused, separate = run(C.PME_XGATHER_AUTO), run(C.PME_XGATHER_OFF)
+    for a, b in zip(fused, separate):
+        assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+        assert a[2] == b[2] and a[3] == b[3] and np.array_equal(a[4], b[4])
+        assert np.array_equal(a[5], b[5])
+    assert np.abs(fused[0][0]).max() > 0
+
+
+def test_x_gather_fusion_rejects_unknown_modes(cuda):
+    from gpu_recip_b200 import CudaPMERecip, _capi as C
+    pme = CudaPMERecip(32, 32, 32, 4)
+    with pytest.raises(C.PMEError) as e:
+        pme.set_x_gather_fusion(7)
+    assert e.value.status == C.PME_EINVAL
