@@ -84,3 +84,18 @@ def test_eval_host_rejects_pageable_memory_and_int64(cuda):
     assert e.value.status == C.PME_EUNSUPPORTED
     with pytest.raises(ValueError):
         pme.eval_host(s.recip9, x_pinned.cuda(), n, s.kappa, True, True, f_pinned, st)
+
+
+def test_eval_host_without_atoms_is_a_no_op(cuda):
+    torch = cuda
+    from gpu_recip_b200 import CudaPMERecip
+    s = S.config_small()
+    pme = CudaPMERecip(*s.nfft, s.order)
+    x = torch.zeros((1, 4), dtype=torch.float32).pin_memory()
+    f = torch.full((3,), 2.0, dtype=torch.float32).pin_memory()
+    pme.energy_virial.clear()
+    pme.eval_host(s.recip9, x, 0, s.kappa, True, True, f, 1)
+    torch.cuda.synchronize()
+    pme.energy_virial.copyToHost()
+    assert pme.energy_virial.getEnergy("recip") == 0.0
+    assert np.all(f.numpy() == 2.0)
