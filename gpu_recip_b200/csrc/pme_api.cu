@@ -144,15 +144,23 @@ int launch_fused_single(pme_recip* h, const SysDesc& d_in) {
   d.bin_atoms = (d.natom + kThreads - 1) / kThreads < sms ? kThreads / 2 : kThreads;
   // inverse x pass inside the gather tiles where its rows fit in the shared memory the other
   // phases already take (so that the launch keeps its CTAs per SM)
+  // (latency build only: the throughput build, for launches with many tiles per CTA, keeps the
+  // separate phase and is compiled without the fused variant)
   d.gx = 0;
   if (h->x_gather == PME_XGATHER_AUTO && gx_smem_bytes(d.g.nx, d.bry, d.brz, d.order) <= fused_smem_bytes(d)) d.gx = 1;
   fused_tile_counts(d, a.total);
-  a.nbar = fused_barriers(a.total);
-  a.single = d;
-  const size_t smem = fused_smem_bytes(d);
+  size_t smem = fused_smem_bytes(d);
   FusedShape shape;
   cudaError_t e = fused_shape(a.total, smem, h->grid_cap, &shape);
+  if (e == cudaSuccess && d.gx && shape.variant != kFusedLatency) {
+    d.gx = 0;
+    fused_tile_counts(d, a.total);
+    smem = fused_smem_bytes(d);
+    e = fused_shape(a.total, smem, h->grid_cap, &shape);
+  }
   if (e != cudaSuccess) return cuda_fail(e, "fused: launch shape (does the kernel fit on an SM?)");
+  a.nbar = fused_barriers(a.total);
+  a.single = d;
   e = fused_launch(a, shape, smem, h->stream);
   if (e != cudaSuccess) return cuda_fail(e, "fused eval launch");
   return PME_OK;

@@ -195,6 +195,7 @@ __device__ __forceinline__ int find_system(const int* prefix, int nsys, int t) {
 }
 
 // The fused evaluation's body; compiled twice (see k_fused_lat / k_fused_tput below).
+template <bool LAT>
 __device__ __forceinline__ void fused_body(const FusedArgs& a) {
   __shared__ SysDesc d;
   __shared__ int cur;
@@ -244,10 +245,15 @@ __device__ __forceinline__ void fused_body(const FusedArgs& a) {
           break;
         default:
           // with the inverse x pass in the gather tiles, the record is finalised by one extra tile here
-          if (d.gx && local == tiles_blocks(d)) {
-            if (threadIdx.x == 0) finalize_system(d, true, true);
+          // (only the latency build has the fused variant; the host never gives gx to the other)
+          if (LAT && d.gx) {
+            if (local == tiles_blocks(d)) {
+              if (threadIdx.x == 0) finalize_system(d, true, true);
+            } else {
+              gather_bin_order<true>(d, local, parity, (char*)smem);
+            }
           } else {
-            gather_bin_dispatch(d, local, parity, (char*)smem);
+            gather_bin_order<false>(d, local, parity, (char*)smem);
           }
           break;
       }
@@ -266,8 +272,8 @@ __device__ __forceinline__ void fused_body(const FusedArgs& a) {
 // tile per CTA in a phase.  Throughput build: at most 80 registers, 3 CTAs per SM (a few spills in
 // the largest tiles); for launches with many tiles per CTA, where the extra resident warps hide
 // more latency than the spills cost.
-__global__ void __launch_bounds__(kThreads) k_fused_lat(const __grid_constant__ FusedArgs a) { fused_body(a); }
-__global__ void __launch_bounds__(kThreads, 3) k_fused_tput(const __grid_constant__ FusedArgs a) { fused_body(a); }
+__global__ void __launch_bounds__(kThreads) k_fused_lat(const __grid_constant__ FusedArgs a) { fused_body<true>(a); }
+__global__ void __launch_bounds__(kThreads, 3) k_fused_tput(const __grid_constant__ FusedArgs a) { fused_body<false>(a); }
 
 // ------------------------------- host launchers ----------------------------------------------
 static size_t staged_fft_smem(int L, int tx) { return tile_smem_bytes(L, tx) + 32 * 7 * sizeof(long long); }

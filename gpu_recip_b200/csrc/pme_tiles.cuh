@@ -1503,10 +1503,6 @@ __device__ __forceinline__ void gather_bin_order(const SysDesc& d, int tile, int
   }
 }
 
-__device__ __forceinline__ void gather_bin_dispatch(const SysDesc& d, int tile, int parity, char* smem) {
-  if (d.gx) gather_bin_order<true>(d, tile, parity, smem);
-  else gather_bin_order<false>(d, tile, parity, smem);
-}
 
 __device__ __forceinline__ void spread_dispatch(const SysDesc& d, int tile, void* smem) {
   switch (d.order) {
