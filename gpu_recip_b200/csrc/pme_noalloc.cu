@@ -1,12 +1,11 @@
 // pme_noalloc.cu -- charge spreading that allocates no device memory.
 //
-// Some callers cannot allocate device memory at the moment they need a charge grid: code that
-// runs while a CUDA stream is being captured into a graph (an allocation there either fails the
-// capture or cannot be replayed), hosts whose own memory manager owns every device byte and
-// forbids plug-ins from calling cudaMalloc behind its back, and time-critical loops that must not
-// take the allocator's locks or synchronise the device.  For them this entry point spreads the
-// charges with the same kernel as pme_spread_charge, but accumulates the exact int64 grid in a
-// fixed device array compiled into this library instead of in memory the library allocates.
+// Some callers cannot allocate device memory at the moment they need a charge grid: hosts whose
+// own memory manager owns every device byte and forbids plug-ins from calling cudaMalloc behind
+// its back, and time-critical loops that must not take the allocator's locks or let an
+// allocation synchronise the device.  For them this entry point spreads the charges with the
+// same kernel as pme_spread_charge, but accumulates the exact int64 grid in a fixed device array
+// compiled into this library instead of in memory the library allocates.
 //
 // The array lives as long as the library is loaded and costs kNoAllocMaxPoints * 8 bytes
 // (8 MiB) on every GPU that loads it.  It is shared by every call: each call clears the part it
@@ -35,25 +34,63 @@ static __device__ __align__(256) unsigned long long g_noalloc_grid[kNoAllocMaxPo
 
 namespace {
 
+// Driver calls reached through the runtime (no link-time dependency on the driver library).
+typedef int (*CtxGetCurrentFn)(void** ctx);
+typedef int (*CtxGetIdFn)(void* ctx, unsigned long long* id);
+
+struct ScratchSlot {
+  unsigned long long ctx_id = 0;   // unique ID of the context the address belongs to (0: none)
+  void* addr = nullptr;
+};
+
 std::mutex g_symbol_mutex;
-void* g_symbol_addr[kMaxDevices] = {nullptr};
+ScratchSlot g_symbol_slot[kMaxDevices];
 
 int noalloc_fail(int status, const std::string& msg) {
   set_last_error(msg.c_str());   // reported by pme_last_error_string()
   return status;
 }
 
-// Device address of the scratch array on the current device, looked up once per device.  In
-// host code the array's name is only a host-side stand-in, never a usable device address.
+// Unique ID of the calling thread's current context (0 when there is none yet).  IDs are never
+// reused within a process, so an address looked up in a context that a device reset destroyed is
+// never taken for one in the context that replaced it.
+unsigned long long current_context_id() {
+  static CtxGetCurrentFn get_current = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = (CtxGetCurrentFn)f;
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = (CtxGetIdFn)f;
+    cudaGetLastError();
+  });
+  void* ctx = nullptr;
+  unsigned long long id = 0;
+  if (!get_current || !get_id || get_current(&ctx) != 0 || ctx == nullptr || get_id(ctx, &id) != 0) return 0;
+  return id;
+}
+
+// Set-up of the scratch array on the current device: its device address, looked up once per
+// device (and again only if the device's context has been replaced, e.g. after cudaDeviceReset).
+// In host code the array's name is only a host-side stand-in, never a usable device address.
 cudaError_t scratch_address(int dev, void** out) {
   std::lock_guard<std::mutex> lock(g_symbol_mutex);
-  if (g_symbol_addr[dev] == nullptr) {
+  ScratchSlot& slot = g_symbol_slot[dev];
+  const unsigned long long id = current_context_id();
+  if (slot.addr == nullptr || id == 0 || id != slot.ctx_id) {
     void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_grid);
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_grid);   // creates the context if needed
     if (e != cudaSuccess) return e;
-    g_symbol_addr[dev] = p;
+    slot.addr = p;
+    slot.ctx_id = current_context_id();
   }
-  *out = g_symbol_addr[dev];
+  *out = slot.addr;
   return cudaSuccess;
 }
 

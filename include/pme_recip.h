@@ -292,15 +292,17 @@ PME_API int pme_server_get_stats(pme_server* s, pme_server_stats* out);
 
 /* ---- spreading without device allocation ----
  * No counterpart in the reference.  For callers that must not allocate device memory when they
- * need a charge grid: code running while a stream is captured into a CUDA graph, hosts whose own
- * memory manager owns all device memory, and latency-critical loops that cannot take allocator
- * locks.  Same spreading kernel and exact int64 fixed-point accumulation as pme_spread_charge,
- * but the accumulation grid is a fixed array compiled into this library (8 MiB on every GPU that
- * loads it, so nfftx*nffty*nfftz <= 1048576; larger grids return PME_EINVAL).  The caller passes
- * the coordinates (device float4[ncoord]), the host recip[9] (orthorhombic: a positive diagonal,
+ * need a charge grid: hosts whose own memory manager owns all device memory and forbids plug-ins
+ * to call cudaMalloc, and latency-critical loops that cannot take allocator locks or let an
+ * allocation synchronise the device.  Same spreading kernel and exact int64 fixed-point
+ * accumulation as pme_spread_charge, but the accumulation grid is a fixed array compiled into
+ * this library (8 MiB on every GPU that loads it, held until the process exits, so
+ * nfftx*nffty*nfftz <= 1048576; larger grids return PME_EINVAL).  The caller passes the
+ * coordinates (device float4[ncoord]), the host recip[9] (orthorhombic: a positive diagonal,
  * off-diagonals return PME_EINVAL) and the output: grid_out, a device float[nfftz][nffty][nfftx]
- * that receives the converted charge grid.  Asynchronous on `stream`.
- * The first call on a device looks up the array's device address (cudaGetSymbolAddress): make it
+ * that receives the converted charge grid.  Asynchronous on `stream`; it calls no cudaMalloc or
+ * cudaFree.  The first call on a device (and the first after that device's context was replaced,
+ * e.g. by cudaDeviceReset) looks up the array's device address (cudaGetSymbolAddress): make it
  * before any stream capture.  All calls share the array and each clears it before use: calls
  * whose work overlaps on the GPU race and corrupt each other's grid. */
 PME_API int pme_spread_charge_noalloc(const void* xyzq, int ncoord, const double* recip, int nfftx,

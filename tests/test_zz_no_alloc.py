@@ -1,8 +1,9 @@
 """GPU test of pme_spread_charge_noalloc, the spreading entry point that allocates no device
-memory (for callers that cannot call cudaMalloc: work captured into CUDA graphs, hosts whose own
-memory manager owns the device, latency-critical loops).  It is compared through the C ABI with
-the existing pme_spread_charge grid, exactly as the other grid tests compare (bit for bit), on
-two calls in a row.  This file is collected last on purpose."""
+memory (for hosts whose own memory manager owns the device and forbids cudaMalloc from plug-ins,
+and for latency-critical loops that cannot take allocator locks).  It is compared through the C ABI
+with the existing pme_spread_charge grid, exactly as the other grid tests compare (bit for bit),
+on two calls in a row, and the device's free memory is checked unchanged around calls after the
+first.  This file is collected last on purpose."""
 import ctypes
 
 import numpy as np
@@ -46,6 +47,25 @@ def test_noalloc_spread_matches_existing_entry_point(cuda):
             torch.cuda.synchronize()
             got = out.cpu().numpy().reshape(nz, ny, nx)
             assert np.array_equal(got, want), (s.name, call, np.abs(got - want).max())
+
+
+def test_noalloc_spread_allocates_no_device_memory(cuda):
+    torch = cuda
+    from gpu_recip_b200 import _capi, recip_from_box
+    lib = _capi.load()
+    s = S.config_small()
+    x = torch.from_numpy(s.xyzq).cuda()
+    nx, ny, nz = s.nfft
+    out = torch.empty(nz * ny * nx, dtype=torch.float32, device="cuda")
+    recip = recip_from_box(s.box)
+    # the first call may load the kernels; the later ones must leave device memory alone
+    assert _noalloc(lib, x, s.natom, recip, s.nfft, s.order, out) == _capi.PME_OK
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for _ in range(3):
+        assert _noalloc(lib, x, s.natom, recip, s.nfft, s.order, out) == _capi.PME_OK
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
 
 
 def test_noalloc_rejects_grids_beyond_its_limit(cuda):
