@@ -36,10 +36,10 @@ sys.path.insert(0, ROOT)
 
 METRIC = "PME recip evals/s at 24k atoms/64^3; batched evals/s + p50/p99 latency, same GPU"
 
-# DRAM bytes (read + write) of one k_fused launch from an ncu capture, by workload (mean of 3
-# launches; profiles/k_fused_water8k_64_p4_full.md).  None where not captured.
-TRAFFIC_BYTES = {"water8k_64_p4": 660139}
 UNIT = "evals/s"
+# DRAM bytes (read + write) per launch of each workload's dominant kernel, from ncu captures kept
+# beside their summaries (each entry names its command); null where a workload was not captured.
+TRAFFIC_FILE = os.path.join(ROOT, "profiles", "dram_traffic.json")
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -63,7 +63,11 @@ def parse():
     ap.add_argument("--reference-gpu-steps", type=int, default=200,
                     help="timed evaluations of the reference's own CUDA operator on this GPU (0: skip)")
     ap.add_argument("--serve-requests", type=int, default=600, help="requests of the serving run (0: skip)")
-    ap.add_argument("--serve-rate", type=float, default=400.0, help="Poisson arrival rate (requests/s)")
+    ap.add_argument("--serve-rate", type=float, default=2000.0, help="Poisson arrival rate (requests/s)")
+    ap.add_argument("--also", nargs="*", default=["water1k_32", "water8k_64_p6"],
+                    help="further single-system workloads timed beside the main one")
+    ap.add_argument("--also-steps", type=int, default=200)
+    ap.add_argument("--no-fft-comparator", dest="fft_comparator", action="store_false")
     return ap.parse_args()
 
 
@@ -90,6 +94,53 @@ def workload_config(s, extra=None):
     if extra:
         cfg.update(extra)
     return cfg
+
+
+def measured_traffic(workload: str):
+    """(bytes per launch, source) of a workload's dominant kernel from the ncu capture record."""
+    try:
+        with open(TRAFFIC_FILE) as fh:
+            rec = json.load(fh).get(workload)
+        if rec:
+            return int(rec["dram_bytes_per_launch"]), rec.get("command")
+    except Exception:
+        pass
+    return None, None
+
+
+def replica_plan(gpus: int, env=None):
+    """What `--gpus N` means for this process: ("spawn", N) when N > 1 and no launcher started the
+    ranks (bench.py then starts N rank processes itself), ("run", world) under a launcher whose
+    world size is N (or N == 1 alone).  A launcher world size other than N is an error."""
+    env = os.environ if env is None else env
+    world = int(env.get("WORLD_SIZE", "0") or 0)
+    if world == 0:
+        return ("spawn", gpus) if gpus > 1 else ("run", 1)
+    if world != gpus:
+        raise SystemExit(f"bench.py: --gpus {gpus} but the launcher started {world} ranks")
+    return ("run", world)
+
+
+def torchrun_command(argv, nproc: int, port: int):
+    """The command that runs this benchmark as nproc rank processes on this node."""
+    return [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={nproc}",
+            "--master-addr=127.0.0.1", f"--master-port={port}", os.path.abspath(__file__)] + list(argv)
+
+
+def spawn_replicas(nproc: int) -> int:
+    import socket
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    return subprocess.call(["timeout", "-k", "60", "3600"] + torchrun_command(sys.argv[1:], nproc, port))
+
+
+def rank_summary(per_rank_ms: float, units: int, world: int, device=None):
+    """Whole-job figures of a timed region: the slowest rank's time (ms) and the rate of all
+    ranks' units over it (units per rank are equal: every replica runs the same workload)."""
+    from gpu_recip_b200 import replicas as R
+    total_ms = R.max_over_ranks(float(per_rank_ms), device)
+    return total_ms, R.aggregate_rate([units] * world, total_ms / 1000.0)
 
 
 def measured_peak():
@@ -302,9 +353,8 @@ def run_b200(args):
     pme.set_energy_virial_mirror(None)
     if not np.isfinite(ev_step.numpy()).all() or ev_step[0].item() == 0.0:
         raise RuntimeError("value: the energy record did not reach the host")
-    total_ms = R.max_over_ranks(float(per.sum()), dev)      # slowest replica
+    total_ms, value = rank_summary(float(per.sum()), K, world, dev)     # slowest replica
     R.barrier()
-    value = R.aggregate_rate([K] * world, total_ms / 1000.0)
 
     # ---- e2e through the C ABI with host buffers -------------------------------------------------
     x_host = torch.from_numpy(s.xyzq).pin_memory()
@@ -329,8 +379,8 @@ def run_b200(args):
     pme.set_energy_virial_mirror(None)
     if not np.isfinite(ev_host.numpy()).all() or ev_host[0].item() == 0.0:
         raise RuntimeError("e2e: the energy record did not reach the host")
-    e_total = R.max_over_ranks(float(sum(e_starts[i].elapsed_time(e_ends[i]) for i in range(Ke))), dev)
-    e2e_value = R.aggregate_rate([Ke] * world, e_total / 1000.0)
+    e_total, e2e_value = rank_summary(float(sum(e_starts[i].elapsed_time(e_ends[i]) for i in range(Ke))), Ke,
+                                      world, dev)
 
     # ---- staged C-ABI calls, per reference stage (informational) -----------------------------------
     stages = stage_times(pme, s, x_dev, f_dev, stride, recip, stream, flush)
@@ -339,13 +389,20 @@ def run_b200(args):
     peak, peak_kind = measured_peak()
     eval_ms = total_ms / K
     achieved = s.alg_bytes() / (eval_ms * 1e-3) / 1e9
+    traffic, traffic_cmd = measured_traffic(args.workload)
     roofline = {"bound": "hbm", "kernel": "k_fused (whole evaluation, one cooperative launch)",
                 "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "peak_source": peak_kind, "traffic": TRAFFIC_BYTES.get(args.workload),
+                "peak_source": peak_kind, "traffic": traffic, "traffic_source": traffic_cmd,
                 "alg_bytes_per_launch": s.alg_bytes(),
-                "staged_stage_us": {k: v * 1000 for k, v in stages.items()}}
+                "staged_stage_us": {k: v * 1000 for k, v in stages.items()},
+                "staged_total_us": 1000 * sum(stages.values())}
 
-    fft_cmp = fft_comparator(s, stages, dev)
+    fft_cmp = fft_comparator(s, dev, flush) if args.fft_comparator else None
+
+    # ---- the other single-system workloads: 3,000 atoms at 32^3 and the production size at order 6
+    others = {}
+    for wname in args.also:
+        others[wname] = run_single(wname, args, dev, stream, flush, rank, world)
 
 
     # ---- batched: uneven systems in one persistent launch --------------------------------------------
@@ -376,7 +433,10 @@ def run_b200(args):
     # ---- the reference's own CUDA operator on this GPU (timing comparator, single GPU only) --------
     reference_gpu = None
     if rank == 0 and world == 1 and args.reference_gpu_steps > 0:
-        reference_gpu = run_reference_gpu(s, args, float(np.percentile(per, 50)) * 1000.0, float(ev_step[0].item()))
+        head = min(n, 4096)
+        f_head = f_dev.view(3, stride)[:, :head].T.cpu().numpy().astype(np.float64)
+        reference_gpu = run_reference_gpu(s, args, float(np.percentile(per, 50)) * 1000.0, float(ev_step[0].item()),
+                                          f_head)
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -399,12 +459,57 @@ def run_b200(args):
                         "d2h_bytes_per_step": 4 * 3 * n + 8 * 11},
                 "gpu_launches": kernels_per_eval * K,
                 "roofline": roofline, "batched": batched, "serving": serving, "large": large,
-                "triclinic": triclinic, "direct": direct,
+                "triclinic": triclinic, "direct": direct, "other_workloads": others,
                 "fft_comparator": fft_cmp, "reference_gpu": reference_gpu,
                 "clocks": clocks.summary(), "cpu_baseline": cpu}
         print(json.dumps(line), flush=True)
     R.barrier()
     R.shutdown()
+
+
+def run_single(name, args, dev, stream, flush, rank, world):
+    """One more single-system workload timed like the main one (fused evaluations, launch shape
+    from the autotuner, L2 flushed before every step), with its roofline and its parity against
+    the FP64 oracle on the same inputs."""
+    import torch
+    from gpu_recip_b200 import CudaPMERecip, force_stride
+    s = make_workload(name, rank)
+    n = s.natom
+    stride = force_stride(n)
+    pme = CudaPMERecip(*s.nfft, s.order, stream=stream)
+    inv_box = [1.0 / b for b in s.box]
+    x = torch.from_numpy(s.xyzq).to(dev)
+    f = torch.zeros(3 * stride, dtype=torch.float32, device=dev)
+    tune = pme.autotune(inv_box, x, n, s.kappa, reps=10)
+    K = args.also_steps
+    W = max(3, args.warmup)
+    e0 = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    e1 = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    with torch.cuda.stream(stream):
+        for i in range(K + W):
+            flush.fill_(float(i & 7))
+            if i >= W:
+                e0[i - W].record(stream)
+            pme.eval_ortho(inv_box, x, n, s.kappa, True, True, f, stride)
+            if i >= W:
+                e1[i - W].record(stream)
+    stream.synchronize()
+    per = np.array([e0[i].elapsed_time(e1[i]) for i in range(K)])
+    total_ms, rate = rank_summary(float(per.sum()), K, world, dev)
+    peak, peak_kind = measured_peak()
+    ms = total_ms / K
+    traffic, traffic_cmd = measured_traffic(name)
+    out = {"workload": workload_config(s)["workload"], "steps": K, "ms_per_eval": ms, "evals_per_s": rate,
+           "p50_ms": float(np.percentile(per, 50)), "p99_ms": float(np.percentile(per, 99)),
+           "alg_bytes_per_eval": s.alg_bytes(),
+           "roofline": {"achieved": s.alg_bytes() / (ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                        "frac": s.alg_bytes() / (ms * 1e-3) / 1e9 / peak, "peak_source": peak_kind,
+                        "traffic": traffic, "traffic_source": traffic_cmd},
+           "launch_shape": {k: tune[k] for k in ("schedule", "x_lines", "y_lines", "z_columns", "grid_ctas")}}
+    if rank == 0:
+        out["gpu_parity"] = workload_parity(pme, s, x, f, stride, inv_box, stream)
+    pme.close()
+    return out
 
 
 def run_batched(args, dev, stream, flush, rank, world):
@@ -422,6 +527,7 @@ def run_batched(args, dev, stream, flush, rank, world):
         st = force_stride(sy.natom)
         f = torch.zeros(3 * st, dtype=torch.float32, device=dev)
         specs.append(dict(nfft=sy.nfft, order=sy.order, box=sy.box, kappa=sy.kappa, xyzq=x, force=f, stride=st))
+    forces = [(sp["force"], sp["stride"]) for sp in specs]
     b = PmeBatch(specs, stream=stream)
     tune = b.autotune(reps=5)
     with torch.cuda.stream(stream):
@@ -449,6 +555,7 @@ def run_batched(args, dev, stream, flush, rank, world):
     per = np.array([st_ev[i].elapsed_time(en_ev[i]) for i in range(K)])
     total = R.max_over_ranks(float(per.sum()), dev)
     del graph
+    parity = batch_parity(systems, forces, b.energy_virial()) if rank == 0 else None
     peak, _ = measured_peak()
     alg = sum(sy.alg_bytes() for sy in systems)
     ms = total / K
@@ -460,7 +567,45 @@ def run_batched(args, dev, stream, flush, rank, world):
             "autotune": {"schedule": ["auto", "planes", "passes"][tune["schedule"]], "grid_ctas": tune["grid_ctas"],
                          "line_scale": tune["x_lines"], "candidates": tune["candidates"]},
             "device_bytes": info["device_bytes"], "alg_bytes_per_batch": alg,
-            "roofline_frac": alg / (ms * 1e-3) / 1e9 / peak}
+            "roofline_frac": alg / (ms * 1e-3) / 1e9 / peak,
+            "traffic": measured_traffic("batch256")[0], "gpu_parity": parity}
+
+
+def parity_subset(systems, count=32, seed=41):
+    """A seeded subset of a batch that includes the smallest and largest atom counts and grids."""
+    natom = np.array([sy.natom for sy in systems])
+    grid = np.array([int(np.prod(sy.nfft)) for sy in systems])
+    keep = {int(natom.argmin()), int(natom.argmax()), int(grid.argmin()), int(grid.argmax())}
+    rest = [i for i in range(len(systems)) if i not in keep]
+    rng = np.random.default_rng(seed)
+    keep.update(int(i) for i in rng.choice(rest, size=min(len(rest), count - len(keep)), replace=False))
+    return sorted(keep)
+
+
+def batch_parity(systems, forces, ev):
+    """The last timed batch evaluation of a subset of systems against the FP64 oracle on the same
+    inputs: worst force relative RMS, energy and virial errors (tolerances 1e-5 / 1e-6 / 1e-5)."""
+    from oracle import oracle as O
+    O.build()
+    worst = {"force_rel_rms": 0.0, "energy_rel": 0.0, "self_energy_rel": 0.0, "virial_rel": 0.0}
+    idx = parity_subset(systems)
+    for i in idx:
+        sy = systems[i]
+        f, st = forces[i]
+        F = f.view(3, st)[:, :sy.natom].T.cpu().numpy().astype(np.float64)
+        ref = O.evaluate(sy.xyzq.astype(np.float64), sy.recip3, sy.nfft, sy.order, sy.kappa)
+        err = {"force_rel_rms": float(np.sqrt(((F - ref["force"]) ** 2).sum() / (ref["force"] ** 2).sum())),
+               "energy_rel": float(abs(ev[i, 0] - ref["energy"]) / abs(ref["energy"])),
+               "self_energy_rel": float(abs(ev[i, 1] - ref["energy_self"]) / abs(ref["energy_self"])),
+               "virial_rel": float(np.abs(ev[i, 2:].reshape(3, 3) - ref["virial"]).max()
+                                   / np.abs(ref["virial"]).max())}
+        for k in worst:
+            worst[k] = max(worst[k], err[k])
+    return {"vs": "FP64 oracle (CPU) on the same inputs", "systems_checked": len(idx),
+            "natom_range": [min(systems[i].natom for i in idx), max(systems[i].natom for i in idx)],
+            "worst": worst, "tolerances": {"force_rel_rms": 1e-5, "energy_rel": 1e-6, "virial_rel": 1e-5},
+            "within_tolerance": bool(worst["force_rel_rms"] <= 1e-5 and worst["energy_rel"] <= 1e-6
+                                     and worst["virial_rel"] <= 1e-5)}
 
 
 def stage_alg_bytes(s):
@@ -521,22 +666,27 @@ def run_large(args, dev, stream, flush, rank, world):
 REF_GPU_BIN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "baseline", "_ref", "ref_gpu_bench")
 
 
-def run_reference_gpu(s, args, b200_us_p50: float, b200_energy: float):
+def run_reference_gpu(s, args, b200_us_p50: float, b200_energy: float, b200_force):
     """Times the reference's own operator, CudaPMERecip<float, float, float2> built from its
     unmodified sources (baseline/ref_gpu), on this GPU and workload: per evaluation the sequence of
     its test driver (record clear, spread, R2C, solve with energy and virial, C2R, gather, self
     energy) with L2 flushed in between, BOX (3-D cuFFT) and COLUMN (1-D cuFFTs and transposes)
-    modes.  It runs as a child process: the reference exits the process on a CUDA error.  Timing
-    only: with CUDA 12.9's cuFFT its in-place transforms no longer get the unpadded layout they
-    were written for, so its results are not valid (reported as result_valid)."""
+    modes.  It runs as a child process: the reference exits the process on a CUDA error.  Its
+    in-place real<->complex transforms run out of place through a scratch copy (the compatibility
+    header's bridge for cuFFT's removed native layout), which adds one grid copy per transform to
+    its time.  Its result is checked against this engine's on the same inputs: energy within the
+    reference driver's own 2e-3 kcal/mol (gpu_recip.cu:146) and the force relative RMS."""
     import struct
     import subprocess
     if not os.path.exists(REF_GPU_BIN):
         return {"unavailable": "baseline/_ref/ref_gpu_bench not built (needs the reference's sources at build time)"}
     out = {"operator": "reference CudaPMERecip<float, float, float2> (gpu_recip), unmodified sources, "
-                       "compiled for sm_100a with compatibility shims", "l2": "flushed (256 MiB memset) before every evaluation"}
+                       "compiled for sm_100a with compatibility shims", "l2": "flushed (256 MiB memset) before every evaluation",
+           "fft_bridge": "in-place R2C/C2R run out of place from a scratch copy (one extra grid copy per transform)"}
+    nforce = int(b200_force.shape[0])
     for ft, name in ((2, "box"), (0, "column")):
-        hdr = struct.pack("<9i4x4d", s.natom, *s.nfft, s.order, ft, 3, args.reference_gpu_steps, 0, s.kappa, *s.box)
+        hdr = struct.pack("<9i4x4d", s.natom, *s.nfft, s.order, ft, 3, args.reference_gpu_steps, nforce, s.kappa,
+                          *s.box)
         try:
             p = subprocess.run([REF_GPU_BIN], input=hdr + np.ascontiguousarray(s.xyzq, dtype=np.float32).tobytes(),
                                capture_output=True, timeout=300)
@@ -548,10 +698,17 @@ def run_reference_gpu(s, args, b200_us_p50: float, b200_energy: float):
             continue
         r = json.loads(p.stdout.decode().strip().splitlines()[-1])
         e = r["energy_recip"]
-        valid = e is not None and abs(e - b200_energy) <= 1e-4 * abs(b200_energy)
+        fh = r.get("force_head") or []
+        f_rms = None
+        if len(fh) == 3 * nforce and all(v is not None for v in fh):
+            fr = np.array(fh, dtype=np.float64).reshape(nforce, 3)
+            f_rms = float(np.sqrt(((fr - b200_force) ** 2).sum() / (b200_force ** 2).sum()))
+        valid = e is not None and abs(e - b200_energy) <= 2e-3 and f_rms is not None and f_rms <= 1e-3
         out[name] = {"us_per_eval_p50": r["us_p50"], "us_per_eval_mean": r["us_mean"], "steps": r["steps"],
-                     "evals_per_s": 1e6 / r["us_mean"], "energy_recip": e, "result_valid": bool(valid),
-                     "b200_speedup_p50": r["us_p50"] / b200_us_p50}
+                     "evals_per_s": 1e6 / r["us_mean"], "energy_recip": e, "energy_b200": b200_energy,
+                     "energy_abs_diff": None if e is None else abs(e - b200_energy),
+                     "force_rel_rms_vs_b200": f_rms, "forces_compared": nforce,
+                     "result_valid": bool(valid), "b200_speedup_p50": r["us_p50"] / b200_us_p50}
     return out
 
 
@@ -682,11 +839,15 @@ def serving_stream(n: int, rate: float, seed: int):
 
 def run_serving(args, dev, rank, world):
     """Requests drawn from the batch distribution (648-24,000 atoms, 24^3-64^3 grids), 1-100
-    evaluations each with 0.05 A Gaussian coordinate jitter, arriving as a Poisson stream: the
-    continuous-batching server against the plain single-system path (one request at a time,
-    first come first served, one cached handle per grid) on the same stream.  Latency = completion
-    - arrival; evals/s = all evaluations / (last completion - first arrival).  Also the server's
-    throughput with every request queued at once."""
+    evaluations each with 0.05 A Gaussian coordinate jitter.  Two arrival patterns over the same
+    request mix: every request queued at once (capacity: the server saturated, against the plain
+    single-system path saturated), and a Poisson stream at --serve-rate (latency under load).  The
+    server is the continuous-batching pme_server_*; the plain path runs one request at a time in
+    arrival order through pme_eval_ortho on one stream, each evaluation's jittered coordinates made
+    on the device and its energy/virial record delivered to pinned host memory by the evaluation
+    itself, with one synchronisation per request (after its last evaluation and the copy of its
+    forces).  Latency = completion - arrival; evals/s = all evaluations / (last completion - first
+    arrival)."""
     import threading
     import torch
     from gpu_recip_b200 import CudaPMERecip, PmeServer
@@ -696,6 +857,7 @@ def run_serving(args, dev, rank, world):
     n = args.serve_requests
     arrivals, idx, nev, seeds = serving_stream(n, args.serve_rate, R.replica_seed(23, rank))
     sigma = 0.05
+    total_evals = float(nev.sum())
 
     def serve(rate_arrivals):
         srv = PmeServer(24 << 30, max_active=256)
@@ -718,75 +880,118 @@ def run_serving(args, dev, rank, world):
         srv.close()
         lat = np.array([r["latency"] for r in res]) * 1000.0
         span = max(r["t_done"] for r in res) - min(r["t_submit"] for r in res)
-        return {"evals_per_s": float(nev.sum()) / span, "p50_ms": float(np.percentile(lat, 50)),
+        return {"evals_per_s": total_evals / span, "p50_ms": float(np.percentile(lat, 50)),
                 "p99_ms": float(np.percentile(lat, 99)), "steps": st["steps"], "seconds": span}
 
-    served = serve(arrivals)
-    saturated = serve(np.zeros(n))
-
-    # plain path: one request at a time in arrival order
+    stream = torch.cuda.Stream(device=dev)
     handles = {}
     xs = [torch.from_numpy(sy.xyzq).to(dev) for sy in pool]
+    cur = [torch.empty_like(x) for x in xs]
+    noise = [torch.empty((sy.natom, 3), dtype=torch.float32, device=dev) for sy in pool]
+    fdev = [torch.empty((sy.natom, 3), dtype=torch.float32, device=dev) for sy in pool]
+    fhost = [torch.empty((sy.natom, 3), dtype=torch.float32).pin_memory() for sy in pool]
+    evh = torch.zeros((int(nev.max()) if n else 1, 11), dtype=torch.float64).pin_memory()
     gen = torch.Generator(device=dev)
-    lat = []
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for i in range(n):
-        wait = t0 + arrivals[i] - time.perf_counter()
-        if wait > 0:
-            time.sleep(wait)
-        sy = pool[idx[i]]
+    for sy in pool:
         key = (tuple(sy.nfft), sy.order)
         if key not in handles:
-            handles[key] = CudaPMERecip(*sy.nfft, sy.order)
-        pme = handles[key]
-        gen.manual_seed(int(seeds[i]) & 0x7FFFFFFF)
-        f = torch.empty((sy.natom, 3), dtype=torch.float32, device=dev)
-        ev = np.zeros((int(nev[i]), 11))
-        for k in range(int(nev[i])):
-            x = xs[idx[i]].clone()
-            x[:, :3] += sigma * torch.randn((sy.natom, 3), generator=gen, device=dev)
-            pme.energy_virial.clear()
-            pme.eval_ortho([1.0 / b for b in sy.box], x, sy.natom, sy.kappa, True, True, f, 1)
-            pme.energy_virial.copyToHost()
-            ev[k, 0] = pme.energy_virial.getEnergy("recip")
-        f.cpu()
-        lat.append((time.perf_counter() - t0 - arrivals[i]) * 1000.0)
-    span = time.perf_counter() - t0
-    plain = {"evals_per_s": float(nev.sum()) / span, "p50_ms": float(np.percentile(lat, 50)),
-             "p99_ms": float(np.percentile(lat, 99)), "seconds": span}
-    total = R.sum_over_ranks(float(nev.sum()), dev)
-    return {"requests": n, "rate_per_s": args.serve_rate, "evals": int(nev.sum()), "sigma_A": sigma,
-            "pool_systems": len(pool), "evals_per_request": "uniform 1-100",
-            "server": served, "server_all_queued": saturated, "plain_path": plain,
+            handles[key] = CudaPMERecip(*sy.nfft, sy.order, stream=stream)
+
+    def plain(rate_arrivals):
+        lat = []
+        count = len(rate_arrivals)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        with torch.cuda.stream(stream):
+            for i in range(count):
+                wait = t0 + rate_arrivals[i] - time.perf_counter()
+                if wait > 0:
+                    time.sleep(wait)
+                j = int(idx[i])
+                sy = pool[j]
+                pme = handles[(tuple(sy.nfft), sy.order)]
+                gen.manual_seed(int(seeds[i]) & 0x7FFFFFFF)
+                for k in range(int(nev[i])):
+                    torch.randn((sy.natom, 3), generator=gen, device=dev, out=noise[j])
+                    cur[j].copy_(xs[j])
+                    cur[j][:, :3].add_(noise[j], alpha=sigma)
+                    pme.set_energy_virial_mirror(evh[k])
+                    pme.eval_ortho([1.0 / b for b in sy.box], cur[j], sy.natom, sy.kappa, True, True, fdev[j], 1)
+                fhost[j].copy_(fdev[j], non_blocking=True)
+                stream.synchronize()
+                lat.append((time.perf_counter() - t0 - rate_arrivals[i]) * 1000.0)
+        span = time.perf_counter() - t0
+        for pme in handles.values():
+            pme.set_energy_virial_mirror(None)
+        return {"evals_per_s": float(nev[:count].sum()) / span, "p50_ms": float(np.percentile(lat, 50)),
+                "p99_ms": float(np.percentile(lat, 99)), "seconds": span}
+
+    plain(np.zeros(min(n, 4)))                      # warm-up of the plain path's handles
+    # capacity: every request queued at once, on the same mix
+    server_cap = serve(np.zeros(n))
+    plain_cap = plain(np.zeros(n))
+    # latency under load: Poisson arrivals at the stated rate
+    server_rate = serve(arrivals)
+    plain_rate = plain(arrivals)
+    arrival_span = float(arrivals[-1]) if n else 0.0
+    total = R.sum_over_ranks(total_evals, dev)
+    for pme in handles.values():
+        pme.close()
+
+    def bound(r):   # the run lasted about as long as the arrivals: its rate is the arrival rate
+        return dict(r, arrival_bound=bool(r["seconds"] < 1.1 * arrival_span + 0.05))
+
+    return {"requests": n, "evals": int(total_evals), "sigma_A": sigma, "pool_systems": len(pool),
+            "evals_per_request": "uniform 1-100",
+            "capacity": {"arrivals": "all requests queued at t = 0", "server": server_cap, "plain_path": plain_cap,
+                         "server_over_plain": server_cap["evals_per_s"] / plain_cap["evals_per_s"]},
+            "at_rate": {"rate_per_s": args.serve_rate, "arrival_span_s": arrival_span,
+                        "server": bound(server_rate), "plain_path": bound(plain_rate)},
             "all_ranks_evals": total}
 
 
-def fft_comparator(s, stages, dev):
-    """cuFFT (torch.fft) 3-D R2C + C2R of the workload's grid, timed like the staged calls, beside
-    this engine's staged r2c_fft + c2r_fft (each of which also converts the fixed-point grid or
-    writes the real grid).  Timing only: cuFFT is never on the product path."""
+def fft_comparator(s, dev, flush, reps: int = 30):
+    """cuFFT (torch.fft) 3-D R2C and C2R beside this engine's staged pme_r2c_fft and pme_c2r_fft
+    (which also convert the fixed-point grid, or write the real grid), each timed with CUDA events
+    and L2 flushed before every transform, on the workload's grid, the 216^3 grid and the
+    smallest, median and largest grids of the 256-system batch.  Timing only: cuFFT is never on
+    the product path."""
     import torch
-    nx, ny, nz = s.nfft
-    g = torch.randn((nz, ny, nx), dtype=torch.float32, device=dev)
-    for _ in range(5):
-        torch.fft.irfftn(torch.fft.rfftn(g), s=(nz, ny, nx))
-    torch.cuda.synchronize()
-    reps = 50
-    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
-    fwd = inv = 0.0
-    for _ in range(reps):
-        e0.record()
+    from gpu_recip_b200 import CudaPMERecip
+    from gpu_recip_b200 import systems as S
+    grids = [tuple(s.nfft), (216, 216, 216)]
+    batch = sorted({tuple(sy.nfft) for sy in S.batch_systems(256, seed=4)}, key=lambda g: g[0] * g[1] * g[2])
+    for g in (batch[0], batch[len(batch) // 2], batch[-1]):
+        if g not in grids:
+            grids.append(g)
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        tot = 0.0
+        for r in range(reps + 3):
+            flush.fill_(float(r & 7))
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            if r >= 3:
+                tot += e0.elapsed_time(e1)
+        return 1000.0 * tot / reps
+
+    out = []
+    for (nx, ny, nz) in grids:
+        g = torch.randn((nz, ny, nx), dtype=torch.float32, device=dev)
         h = torch.fft.rfftn(g)
-        e1.record()
-        torch.fft.irfftn(h, s=(nz, ny, nx))
-        e2.record()
-        torch.cuda.synchronize()
-        fwd += e0.elapsed_time(e1)
-        inv += e1.elapsed_time(e2)
-    return {"cufft_r2c_us": 1000 * fwd / reps, "cufft_c2r_us": 1000 * inv / reps,
-            "b200_r2c_fft_us": 1000 * stages["r2c_fft"], "b200_c2r_fft_us": 1000 * stages["c2r_fft"],
-            "note": "cuFFT timed as a comparator only (torch.fft); L2 warm for both"}
+        pme = CudaPMERecip(nx, ny, nz, 4)
+        row = {"grid": [nx, ny, nz],
+               "cufft_r2c_us": timed(lambda: torch.fft.rfftn(g)),
+               "cufft_c2r_us": timed(lambda: torch.fft.irfftn(h, s=(nz, ny, nx))),
+               "b200_r2c_fft_us": timed(pme.r2c_fft),
+               "b200_c2r_fft_us": timed(pme.c2r_fft)}
+        pme.close()
+        out.append(row)
+    return {"grids": out, "l2": "flushed (256 MiB write) before every transform, both arms",
+            "note": "cuFFT timed as a comparator only (torch.fft)"}
 
 
 def stage_times(pme, s, x, f, stride, recip, stream, flush, reps: int = 50):
@@ -814,6 +1019,9 @@ def stage_times(pme, s, x, f, stride, recip, stream, flush, reps: int = 50):
 
 def main():
     args = parse()
+    mode, n = replica_plan(args.gpus)
+    if mode == "spawn":
+        sys.exit(spawn_replicas(n))
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -6,11 +6,11 @@ interface (CudaPMERecip / CudaDomdecRecip of ap-hynninen/gpu_recip).
 """
 from . import _capi
 from .pme import (CCELEC, FFT_BOX, FFT_COLUMN, FFT_SLAB, FORCE_SCALE, CudaDomdecRecip,
-                  CudaPMERecip, EnergyVirial, PmeBatch, PmeServer, force_stride, recip_from_box,
-                  recip_from_box_vectors, system_device_bytes)
+                  CudaPMERecip, EnergyVirial, PmeBatch, PmeServer, force_convert, force_convert_add,
+                  force_stride, recip_from_box, recip_from_box_vectors, system_device_bytes)
 
 __all__ = ["CudaPMERecip", "CudaDomdecRecip", "EnergyVirial", "PmeBatch", "PmeServer", "recip_from_box",
-           "recip_from_box_vectors", "force_stride", "system_device_bytes",
+           "recip_from_box_vectors", "force_stride", "force_convert", "force_convert_add", "system_device_bytes",
            "FFT_BOX", "FFT_COLUMN", "FFT_SLAB", "CCELEC", "FORCE_SCALE", "load_library"]
 
 

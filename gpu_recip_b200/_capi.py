@@ -76,6 +76,8 @@ SIGNATURES = {
     "pme_system_device_bytes": [_I, _I, _I],
     "pme_set_trace": [_P, _P, _I],
     "pme_spread_charge_noalloc": [_P, _I, _DP, _I, _I, _I, _I, _P, _P],
+    "pme_force_convert": [_P, _I, _I, _P, _I, _I, _P],
+    "pme_force_convert_add": [_P, _I, _I, _P, _I, _I, _P],
     "pme_batch_set_trace": [_P, _P, _I],
     "pme_autotune": [_P, _P, _I, _D, _D, _D, _D, _I, _P],
     "pme_get_tune_config": [_P, _P],
@@ -112,6 +114,7 @@ _RESTYPES = {"pme_last_error_string": ctypes.c_char_p, "pme_status_string": ctyp
 PME_INJECT_NONE, PME_INJECT_SKIP_BARRIER = 0, 1
 PME_SCHED_AUTO, PME_SCHED_PLANES, PME_SCHED_PASSES = 0, 1, 2
 PME_XGATHER_AUTO, PME_XGATHER_OFF = 0, 1
+PME_REAL_F32, PME_REAL_F64 = 0, 1
 
 
 class SystemDesc(ctypes.Structure):

@@ -45,11 +45,31 @@ def _stale() -> bool:
 
 
 def build(force: bool = False, verbose: bool = False, extra=None) -> str:
+    """Compile every csrc/*.cu to an object in parallel (nvcc per file), then link the .so."""
     if not force and not _stale():
         return LIB
+    from concurrent.futures import ThreadPoolExecutor
+    objdir = os.path.join(PKG, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    srcs = sources()
+    objs = [os.path.join(objdir, os.path.basename(f)[:-3] + ".o") for f in srcs]
+
+    def compile_one(pair):
+        src, obj = pair
+        cmd = [nvcc()] + ARCH + NVCC_FLAGS + list(extra or []) + ["-c", src, "-o", obj]
+        if verbose:
+            print(" ".join(cmd))
+        return subprocess.run(cmd, capture_output=True, text=True)
+
+    with ThreadPoolExecutor(max_workers=max(1, min(len(srcs), os.cpu_count() or 1))) as ex:
+        results = list(ex.map(compile_one, zip(srcs, objs)))
+    for src, r in zip(srcs, results):
+        if r.stdout or r.stderr:
+            sys.stderr.write(r.stdout + r.stderr)
+        if r.returncode != 0:
+            raise subprocess.CalledProcessError(r.returncode, f"nvcc {src}")
     tmp = LIB + ".tmp"
-    cmd = [nvcc()] + ARCH + NVCC_FLAGS + list(extra or []) + ["-shared", "-o", tmp] + sources()
-    cmd += ["-Xlinker", "--exclude-libs,ALL"]
+    cmd = [nvcc()] + ARCH + ["-shared", "-o", tmp] + objs + ["-Xlinker", "--exclude-libs,ALL"]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)

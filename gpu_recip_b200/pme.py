@@ -466,6 +466,44 @@ class PmeBatch:
         return {"nsys": n.value, "grid_ctas": g.value, "device_bytes": b.value}
 
 
+def _real_type(t) -> int:
+    import torch
+    if t.dtype == torch.float64:
+        return C.PME_REAL_F64
+    if t.dtype == torch.float32:
+        return C.PME_REAL_F32
+    raise ValueError("float32 or float64 force array expected")
+
+
+def force_convert(force_i64, stride: int, ncoord: int, out=None, out_stride: Optional[int] = None, stream=None):
+    """Force<long long>::convert (Force.cu:103-157): int64 SoA forces at 2^40 (rows of ``stride``)
+    to float32 or float64 SoA rows of ``out_stride`` in ``out``; with ``out`` None the conversion
+    is in place to float64 and the float64 view of the same storage is returned (convert<double>(),
+    as CudaPMEForcefield.cu:514 does at the end of an MD step)."""
+    import torch
+    if force_i64.dtype != torch.int64:
+        raise ValueError("int64 fixed-point force array expected")
+    if out is None:
+        out, out_stride = force_i64.view(torch.float64), stride
+    if out_stride is None:
+        out_stride = stride
+    C.check(C.load().pme_force_convert(_ptr(force_i64), int(stride), int(ncoord), _ptr(out), int(out_stride),
+                                       _real_type(out), _stream_handle(stream)), "force_convert")
+    return out
+
+
+def force_convert_add(force_i64, stride: int, ncoord: int, add, add_stride: Optional[int] = None, stream=None):
+    """Force<long long>::convert_add (Force.cu:167-184): in place, int64 SoA forces at 2^40 become
+    float64 v 2^-40 + add (float32 or float64 SoA rows); returns the float64 view."""
+    import torch
+    if force_i64.dtype != torch.int64:
+        raise ValueError("int64 fixed-point force array expected")
+    C.check(C.load().pme_force_convert_add(_ptr(force_i64), int(stride), int(ncoord), _ptr(add),
+                                           int(add_stride if add_stride is not None else stride), _real_type(add),
+                                           _stream_handle(stream)), "force_convert_add")
+    return force_i64.view(torch.float64)
+
+
 def system_device_bytes(nfft) -> int:
     return int(C.load().pme_system_device_bytes(int(nfft[0]), int(nfft[1]), int(nfft[2])))
 

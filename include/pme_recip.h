@@ -126,6 +126,25 @@ PME_API int pme_eval_host(pme_recip* h, const double* recip, const void* xyzq_ho
                           double kappa, int calc_energy, int calc_virial, int kind, void* force_host,
                           int stride);
 
+/* ---- fixed-point force conversion (Force<long long>, Force.cu:103-190) ----
+ * An MD step accumulates reciprocal (PME_FORCE_I64_SOA_ACCUM), direct and 1-4 forces into one
+ * int64 SoA array at scale 2^40 and converts it once (CudaPMEForcefield.cu:514).  Every value
+ * becomes the int64 rounded once to the output type times 2^-40 (exact), i.e. the reference's
+ * ((T)v) * INV_FORCE_SCALE (reduce.cu:15-53).  Only the ncoord entries of each of the three rows
+ * are read and written (stride padding is left alone).  Asynchronous on `stream`. */
+enum { PME_REAL_F32 = 0, PME_REAL_F64 = 1 };
+/* Force<long long>::convert<T2>(Force<T2>&) (Force.cu:103-128): rows at in + k in_stride to rows
+ * at out + k out_stride of out_type.  out == in converts in place (PME_REAL_F64 and the same
+ * stride only), as Force<long long>::convert<double>() (Force.cu:143-157); other overlaps are
+ * PME_EINVAL. */
+PME_API int pme_force_convert(const long long* in, int in_stride, int ncoord, void* out, int out_stride,
+                              int out_type, void* stream);
+/* Force<long long>::convert_add<double, T>(Force<T>&) (Force.cu:167-184, reduce.cu:152-170): in
+ * place, each int64 entry v of inout becomes the double v 2^-40 + add, with add float or double
+ * (add_type) SoA rows at add + k add_stride. */
+PME_API int pme_force_convert_add(long long* inout, int stride, int ncoord, const void* add, int add_stride,
+                                  int add_type, void* stream);
+
 /* ---- grid read-back for parity checks (synchronise the stream; host outputs) ----
  * Layouts follow the reference: real grids [z][y][x]; half-complex grid [z][y][kx],
  * kx = 0..nfftx/2, interleaved (re, im). */

@@ -43,6 +43,67 @@ def test_domdec_recip_three_force_kinds_and_int64_accumulate(cuda):
     assert np.array_equal(got, want)
 
 
+def test_int64_accumulate_then_convert_as_the_md_step(cuda):
+    """The end of an MD step (CudaPMEForcefield.cu:514): reciprocal forces accumulated in int64
+    onto forces already there, then Force<long long>::convert to double (in place and out of
+    place), to float, and convert_add of a float force array: every value is the accumulated
+    int64 rounded once to the type times 2^-40, bit for bit."""
+    torch = cuda
+    from gpu_recip_b200 import CudaDomdecRecip, force_convert, force_convert_add, force_stride
+    s = S.config_small(seed=7)
+    n = s.natom
+    rec = CudaDomdecRecip(*s.nfft, s.order, s.kappa)
+    x = torch.from_numpy(s.xyzq).cuda()
+    inv = [1.0 / b for b in s.box]
+    f3 = torch.zeros((n, 3), dtype=torch.float32, device="cuda")
+    rec.calc(*inv, x, n, True, True, f3)
+    st8 = force_stride(n, 8)
+    prior = np.random.default_rng(4).integers(-2 ** 45, 2 ** 45, size=(3, st8)).astype(np.int64)
+    fi = torch.from_numpy(prior.copy().reshape(-1)).cuda()
+    rec.calc(*inv, x, n, True, True, fi, st8)
+    torch.cuda.synchronize()
+    acc = prior.copy()
+    acc[:, :n] += _fixed(f3.cpu().numpy()).T          # prior + rint(F 2^40)
+    assert np.array_equal(fi.view(3, st8).cpu().numpy(), acc)
+    want64 = acc[:, :n].astype(np.float64) * 2.0 ** -40
+    want32 = acc[:, :n].astype(np.float32) * np.float32(2.0 ** -40)
+    # out of place, other strides; the padding of the output is left alone
+    so = force_stride(n, 8) + 64
+    out64 = torch.full((3 * so,), -7.0, dtype=torch.float64, device="cuda")
+    force_convert(fi, st8, n, out64, so)
+    out32 = torch.full((3 * so,), -7.0, dtype=torch.float32, device="cuda")
+    force_convert(fi, st8, n, out32, so)
+    torch.cuda.synchronize()
+    o64 = out64.view(3, so).cpu().numpy()
+    o32 = out32.view(3, so).cpu().numpy()
+    assert np.array_equal(o64[:, :n], want64) and np.all(o64[:, n:] == -7.0)
+    assert np.array_equal(o32[:, :n], want32) and np.all(o32[:, n:] == -7.0)
+    # convert_add of a float32 array (the reference's reduce_add_force<long long, double, float>)
+    add = torch.from_numpy(np.random.default_rng(5).standard_normal((3, st8)).astype(np.float32).reshape(-1)).cuda()
+    fa = fi.clone()
+    d = force_convert_add(fa, st8, n, add)
+    # in place: convert<double>() of the int64 array itself
+    d2 = force_convert(fi, st8, n)
+    torch.cuda.synchronize()
+    assert np.array_equal(d2.view(3, st8)[:, :n].cpu().numpy(), want64)
+    want_add = want64 + add.view(3, st8)[:, :n].cpu().numpy().astype(np.float64)
+    assert np.array_equal(d.view(3, st8)[:, :n].cpu().numpy(), want_add)
+
+
+def test_force_convert_rejects_bad_arguments(cuda):
+    torch = cuda
+    from gpu_recip_b200 import _capi, force_convert
+    fi = torch.zeros(3 * 64, dtype=torch.int64, device="cuda")
+    f32 = fi.view(torch.float64)[:96].view(torch.float32)   # overlaps fi
+    with pytest.raises(_capi.PMEError):
+        force_convert(fi, 64, 32, f32, 64)                  # overlapping float output
+    with pytest.raises(_capi.PMEError):
+        force_convert(fi, 64, 65)                           # ncoord beyond the stride
+    out = torch.zeros(3 * 64, dtype=torch.float32, device="cuda")
+    with pytest.raises(_capi.PMEError):
+        force_convert(fi, 64, 32, out, 16)                  # output stride below ncoord
+
+
 def test_recip_looper_serves_a_direct_node(cuda):
     torch = cuda
     from gpu_recip_b200 import CudaDomdecRecip

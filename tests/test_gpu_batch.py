@@ -156,3 +156,54 @@ def test_barrier_timeout_is_reported_not_hung(cuda):
     pme.energy_virial.copyToHost()
     assert np.array_equal(f.view(3, stride)[:, : s.natom].T.cpu().numpy(), eager[0])
     assert pme.energy_virial.getEnergy("recip") == eager[1]
+
+
+def test_benched_256_system_batch_matches_oracle(cuda, oracle):
+    """The batched workload exactly as the benchmark times it: 256 water boxes of 648-24,000 atoms
+    and 24^3-64^3 grids (seed 4), the launch shape picked by the batch autotuner, the step replayed
+    from a CUDA graph.  A seeded subset of 32 systems (with the smallest and largest atom counts
+    and grids, chosen as the benchmark's own parity block chooses them) against the FP64 oracle;
+    every system's energy is finite."""
+    torch = cuda
+    import bench
+    from gpu_recip_b200 import PmeBatch, force_stride
+    systems = S.batch_systems(256, seed=4)
+    specs, fs = [], []
+    for s in systems:
+        x = torch.from_numpy(s.xyzq).cuda()
+        stride = force_stride(s.natom)
+        f = torch.zeros(3 * stride, dtype=torch.float32, device="cuda")
+        fs.append((f, stride))
+        specs.append(dict(nfft=s.nfft, order=s.order, box=s.box, kappa=s.kappa, xyzq=x, force=f, stride=stride))
+    stream = torch.cuda.Stream()
+    b = PmeBatch(specs, stream=stream)
+    tune = b.autotune(reps=3)
+    assert tune["candidates"] >= 1
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=stream):
+        b.clear_energy_virial()
+        b.eval()
+    for f, _ in fs:
+        f.zero_()
+    torch.cuda.synchronize()
+    graph.replay()
+    torch.cuda.synchronize()
+    ev = b.energy_virial()
+    del graph
+    assert np.all(np.isfinite(ev))
+    idx = bench.parity_subset(systems)
+    assert len(idx) == 32
+    natoms = [s.natom for s in systems]
+    assert natoms.index(min(natoms)) in idx and natoms.index(max(natoms)) in idx
+    for i in idx:
+        s = systems[i]
+        f, stride = fs[i]
+        F = f.view(3, stride)[:, : s.natom].T.cpu().numpy().astype(np.float64)
+        ref = oracle.evaluate(s.xyzq.astype(np.float64), s.recip3, s.nfft, s.order, s.kappa)
+        rms = np.sqrt(((F - ref["force"]) ** 2).sum() / (ref["force"] ** 2).sum())
+        assert rms <= 1e-5, (s.name, s.natom, s.nfft, rms)
+        assert abs(ev[i, 0] - ref["energy"]) <= 1e-6 * abs(ref["energy"]), (s.name, ev[i, 0], ref["energy"])
+        assert abs(ev[i, 1] - ref["energy_self"]) <= 1e-12 * abs(ref["energy_self"]), s.name
+        vir = ev[i, 2:].reshape(3, 3)
+        assert np.abs(vir - ref["virial"]).max() <= 1e-5 * np.abs(ref["virial"]).max(), s.name
+

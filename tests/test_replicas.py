@@ -62,3 +62,49 @@ def test_max_over_ranks_gloo_two_ranks():
         p.join(timeout=60)
         assert p.exitcode == 0
     assert res == [(0, 2.0, 10.0), (1, 2.0, 10.0)]
+
+
+def test_bench_gpus_flag_means_replicas():
+    """`bench.py --gpus N` starts N rank processes itself unless a launcher already did; a
+    launcher world size other than N is refused."""
+    import bench
+    assert bench.replica_plan(1, {}) == ("run", 1)
+    assert bench.replica_plan(4, {}) == ("spawn", 4)
+    assert bench.replica_plan(2, {"WORLD_SIZE": "2"}) == ("run", 2)
+    assert bench.replica_plan(1, {"WORLD_SIZE": "1"}) == ("run", 1)
+    with pytest.raises(SystemExit):
+        bench.replica_plan(8, {"WORLD_SIZE": "2"})
+    cmd = bench.torchrun_command(["--gpus", "2", "--steps", "5"], 2, 29555)
+    assert cmd[1:3] == ["-m", "torch.distributed.run"]
+    assert "--nproc-per-node=2" in cmd and "--master-addr=127.0.0.1" in cmd and "--master-port=29555" in cmd
+    assert cmd[-4:] == ["--gpus", "2", "--steps", "5"] and cmd[-5].endswith("bench.py")
+
+
+def _bench_worker(rank, world, port, out):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank),
+                      WORLD_SIZE=str(world), LOCAL_RANK=str(rank))
+    import bench
+    assert bench.replica_plan(world) == ("run", world)
+    assert R.init("gloo", timeout_s=60)
+    # rank r timed 10 (r + 1) ms for 100 evaluations: the job took the slowest rank's 20 ms and
+    # did 200 evaluations
+    total_ms, value = bench.rank_summary(10.0 * (rank + 1), 100, world)
+    R.shutdown()
+    out.put((rank, total_ms, value))
+
+
+def test_bench_rank_summary_gloo_two_ranks():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    ps = [ctx.Process(target=_bench_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in ps:
+        p.start()
+    res = sorted(q.get(timeout=120) for _ in ps)
+    for p in ps:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert [r[0] for r in res] == [0, 1]
+    for _, total_ms, value in res:
+        assert total_ms == 20.0 and abs(value - 200 / 0.020) < 1e-6
+
