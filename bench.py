@@ -435,8 +435,11 @@ def run_b200(args):
     if rank == 0 and world == 1 and args.reference_gpu_steps > 0:
         head = min(n, 4096)
         f_head = f_dev.view(3, stride)[:, :head].T.cpu().numpy().astype(np.float64)
+        from oracle import oracle as O
+        O.build()
+        ref = O.evaluate(s.xyzq.astype(np.float64), s.recip3, s.nfft, s.order, s.kappa)
         reference_gpu = run_reference_gpu(s, args, float(np.percentile(per, 50)) * 1000.0, float(ev_step[0].item()),
-                                          f_head)
+                                          f_head, {"energy": float(ref["energy"]), "force_head": ref["force"][:head]})
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -666,7 +669,7 @@ def run_large(args, dev, stream, flush, rank, world):
 REF_GPU_BIN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "baseline", "_ref", "ref_gpu_bench")
 
 
-def run_reference_gpu(s, args, b200_us_p50: float, b200_energy: float, b200_force):
+def run_reference_gpu(s, args, b200_us_p50: float, b200_energy: float, b200_force, fp64):
     """Times the reference's own operator, CudaPMERecip<float, float, float2> built from its
     unmodified sources (baseline/ref_gpu), on this GPU and workload: per evaluation the sequence of
     its test driver (record clear, spread, R2C, solve with energy and virial, C2R, gather, self
@@ -674,8 +677,13 @@ def run_reference_gpu(s, args, b200_us_p50: float, b200_energy: float, b200_forc
     modes.  It runs as a child process: the reference exits the process on a CUDA error.  Its
     in-place real<->complex transforms run out of place through a scratch copy (the compatibility
     header's bridge for cuFFT's removed native layout), which adds one grid copy per transform to
-    its time.  Its result is checked against this engine's on the same inputs: energy within the
-    reference driver's own 2e-3 kcal/mol (gpu_recip.cu:146) and the force relative RMS."""
+    its time.  Its result is checked against the FP64 oracle on the same inputs (fp64: energy and
+    the forces of the first atoms): energy within the reference driver's own 2e-3 kcal/mol
+    (gpu_recip.cu:146) and forces within its 1e-3 kcal/mol/A (gpu_recip.cu:286-287); this engine's
+    differences from the same values are beside them.  In COLUMN mode the reference applies its
+    x-mirror energy doubling to the z axis (CudaPMERecip.cu:708-742 run with nfft1 = nfftz,
+    :1977-1988), so its COLUMN energy differs by design of that code path; its own test drives
+    BOX only (gpu_recip.cu:80), and COLUMN is judged by its forces."""
     import struct
     import subprocess
     if not os.path.exists(REF_GPU_BIN):
@@ -699,16 +707,25 @@ def run_reference_gpu(s, args, b200_us_p50: float, b200_energy: float, b200_forc
         r = json.loads(p.stdout.decode().strip().splitlines()[-1])
         e = r["energy_recip"]
         fh = r.get("force_head") or []
-        f_rms = None
+        f_max = f_rms = None
+        ff = fp64["force_head"]
         if len(fh) == 3 * nforce and all(v is not None for v in fh):
             fr = np.array(fh, dtype=np.float64).reshape(nforce, 3)
-            f_rms = float(np.sqrt(((fr - b200_force) ** 2).sum() / (b200_force ** 2).sum()))
-        valid = e is not None and abs(e - b200_energy) <= 2e-3 and f_rms is not None and f_rms <= 1e-3
+            f_max = float(np.abs(fr - ff).max())
+            f_rms = float(np.sqrt(((fr - ff) ** 2).sum() / (ff ** 2).sum()))
+        e_ok = e is not None and abs(e - fp64["energy"]) <= 2e-3
+        f_ok = f_max is not None and f_max <= 1e-3
         out[name] = {"us_per_eval_p50": r["us_p50"], "us_per_eval_mean": r["us_mean"], "steps": r["steps"],
-                     "evals_per_s": 1e6 / r["us_mean"], "energy_recip": e, "energy_b200": b200_energy,
-                     "energy_abs_diff": None if e is None else abs(e - b200_energy),
-                     "force_rel_rms_vs_b200": f_rms, "forces_compared": nforce,
-                     "result_valid": bool(valid), "b200_speedup_p50": r["us_p50"] / b200_us_p50}
+                     "evals_per_s": 1e6 / r["us_mean"],
+                     "energy_recip": e, "energy_fp64": fp64["energy"], "energy_b200": b200_energy,
+                     "energy_abs_diff_vs_fp64": None if e is None else abs(e - fp64["energy"]),
+                     "b200_energy_abs_diff_vs_fp64": abs(b200_energy - fp64["energy"]),
+                     "force_max_abs_diff_vs_fp64": f_max, "force_rel_rms_vs_fp64": f_rms,
+                     "b200_force_max_abs_diff_vs_fp64": float(np.abs(b200_force - ff).max()),
+                     "b200_force_rel_rms_vs_fp64": float(np.sqrt(((b200_force - ff) ** 2).sum() / (ff ** 2).sum())),
+                     "forces_compared": nforce, "energy_valid": bool(e_ok), "forces_valid": bool(f_ok),
+                     "result_valid": bool(f_ok and (e_ok or name == "column")),
+                     "b200_speedup_p50": r["us_p50"] / b200_us_p50}
     return out
 
 
