@@ -45,7 +45,6 @@ struct pme_recip {
   char* d_block = nullptr;
   unsigned long long* d_bar = nullptr;
   int* d_status = nullptr;
-  bool accum_dirty = false;
   size_t max_smem = 0;
   unsigned int spin_limit = 1u << 22;
   int inject = 0;
@@ -93,6 +92,14 @@ void release(pme_recip* h) {
 }
 
 int handle_ok(const pme_recip* h) { return h ? PME_OK : fail(PME_EINVAL, "handle is NULL"); }
+
+// Barrier words of a handle: [0] arrival counter, [1] its value at launch start, [2] device status
+// (int), [3] launch counter (bin parity), [4] arrival counter of the self-energy launch.
+constexpr int kBarWords = 6;
+
+StagedCtx staged_ctx(const pme_recip* h) { return StagedCtx{h->d_bar, h->d_status, h->spin_limit}; }
+
+unsigned int* self_counter(const pme_recip* h) { return (unsigned int*)(h->d_bar + 4); }
 
 // Size the fused path's atom bins for natom atoms (allocates only when the count grows).
 int ensure_bins(pme_recip* h, int natom) {
@@ -244,7 +251,7 @@ int pme_create(int nfftx, int nffty, int nfftz, int order, int fft_type, int nno
   apply_cached_config(h);
   const size_t bytes = SystemState::bytes(nfftx, nffty, nfftz);
   if (cudaMalloc(&h->d_block, bytes) != cudaSuccess ||
-      cudaMalloc(&h->d_bar, 4 * sizeof(unsigned long long)) != cudaSuccess) {
+      cudaMalloc(&h->d_bar, kBarWords * sizeof(unsigned long long)) != cudaSuccess) {
     cudaGetLastError();
     release(h);
     return fail(PME_ENOMEM, "device allocation failed");
@@ -252,7 +259,7 @@ int pme_create(int nfftx, int nffty, int nfftz, int order, int fft_type, int nno
   h->d_status = (int*)(h->d_bar + 2);
   h->st.carve(h->d_block);
   e = cudaMemset(h->d_block, 0, bytes);
-  if (e == cudaSuccess) e = cudaMemset(h->d_bar, 0, 4 * sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMemset(h->d_bar, 0, kBarWords * sizeof(unsigned long long));
   if (e == cudaSuccess) e = h->st.upload_tables();
   if (e != cudaSuccess) {
     release(h);
@@ -322,20 +329,22 @@ int pme_spread_charge(pme_recip* h, const void* xyzq, int ncoord, const double* 
   if (ncoord < 0 || (ncoord > 0 && !xyzq)) return fail(PME_EINVAL, "bad xyzq/ncoord");
   if (int rc = check_recip(recip)) return rc;
   DeviceGuard dg(h->device);
-  cudaError_t e = cudaMemsetAsync(h->st.accum, 0, h->st.G() * 8, h->stream);
-  if (e != cudaSuccess) return cuda_fail(e, "spread_charge: clear grid");
-  e = staged_spread(h->st.desc9(recip, 0.0, xyzq, ncoord, nullptr, 0, 0, 0, 0), h->stream);
+  if (int rc = ensure_bins(h, ncoord)) return rc;
+  // bin by row block, then each block's exact rows to the int64 grid (every point is written)
+  SysDesc d = h->st.desc9(recip, 0.0, xyzq, ncoord, nullptr, 0, 0, 0, 0);
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
+  d.bin_atoms = (ncoord + kThreads - 1) / kThreads < sms ? kThreads / 2 : kThreads;
+  cudaError_t e = staged_spread_binned(d, staged_ctx(h), h->stream);
   if (e != cudaSuccess) return cuda_fail(e, "spread_charge");
-  h->accum_dirty = true;
   return PME_OK;
 }
 
 int pme_r2c_fft(pme_recip* h) {
   if (int rc = handle_ok(h)) return rc;
   DeviceGuard dg(h->device);
-  cudaError_t e = staged_r2c(h->st.desc(nullptr, 0.0, nullptr, 0, nullptr, 0, 0, 0, 0), true, h->stream);
+  cudaError_t e = staged_r2c(h->st.desc(nullptr, 0.0, nullptr, 0, nullptr, 0, 0, 0, 0), staged_ctx(h), h->stream);
   if (e != cudaSuccess) return cuda_fail(e, "r2c_fft");
-  h->accum_dirty = false;
   return PME_OK;
 }
 
@@ -345,7 +354,7 @@ int pme_scalar_sum(pme_recip* h, const double* recip, double kappa, int calc_ene
   if (!(kappa > 0.0) || !std::isfinite(kappa)) return fail(PME_EINVAL, "kappa must be positive");
   DeviceGuard dg(h->device);
   const int ev = (calc_energy || calc_virial) ? 1 : 0;
-  cudaError_t e = staged_solve(h->st.desc9(recip, kappa, nullptr, 0, nullptr, 0, 0, ev, 0), h->stream);
+  cudaError_t e = staged_solve(h->st.desc9(recip, kappa, nullptr, 0, nullptr, 0, 0, ev, 0), staged_ctx(h), h->stream);
   if (e != cudaSuccess) return cuda_fail(e, "scalar_sum");
   return PME_OK;
 }
@@ -353,7 +362,7 @@ int pme_scalar_sum(pme_recip* h, const double* recip, double kappa, int calc_ene
 int pme_c2r_fft(pme_recip* h) {
   if (int rc = handle_ok(h)) return rc;
   DeviceGuard dg(h->device);
-  cudaError_t e = staged_c2r(h->st.desc(nullptr, 0.0, nullptr, 0, nullptr, 0, 0, 0, 0), h->stream);
+  cudaError_t e = staged_c2r(h->st.desc(nullptr, 0.0, nullptr, 0, nullptr, 0, 0, 0, 0), staged_ctx(h), h->stream);
   if (e != cudaSuccess) return cuda_fail(e, "c2r_fft");
   return PME_OK;
 }
@@ -375,7 +384,7 @@ int pme_calc_self_energy(pme_recip* h, const void* xyzq, int ncoord, double kapp
   if (ncoord < 0 || (ncoord > 0 && !xyzq)) return fail(PME_EINVAL, "bad xyzq/ncoord");
   if (!std::isfinite(kappa)) return fail(PME_EINVAL, "kappa must be finite");
   DeviceGuard dg(h->device);
-  cudaError_t e = staged_self(h->st.desc(nullptr, kappa, xyzq, ncoord, nullptr, 0, 0, 0, 1), h->stream);
+  cudaError_t e = staged_self(h->st.desc(nullptr, kappa, xyzq, ncoord, nullptr, 0, 0, 0, 1), self_counter(h), h->stream);
   if (e != cudaSuccess) return cuda_fail(e, "calc_self_energy");
   return PME_OK;
 }
@@ -448,11 +457,6 @@ int pme_eval(pme_recip* h, const double* recip, const void* xyzq, int ncoord, do
   if (!(kappa > 0.0) || !std::isfinite(kappa)) return fail(PME_EINVAL, "kappa must be positive");
   if (int rc = check_force_args(ncoord, stride, kind, force)) return rc;
   DeviceGuard dg(h->device);
-  if (h->accum_dirty) {   // a staged spread_charge is pending: start from an empty grid
-    cudaError_t e = cudaMemsetAsync(h->st.accum, 0, h->st.G() * 8, h->stream);
-    if (e != cudaSuccess) return cuda_fail(e, "eval: clear grid");
-    h->accum_dirty = false;
-  }
   if (int rc = ensure_bins(h, ncoord)) return rc;
   const int ev = (calc_energy || calc_virial) ? 1 : 0;
   SysDesc d = h->st.desc9(recip, kappa, xyzq, ncoord, force, kind, stride, ev, calc_energy ? 1 : 0);
@@ -502,11 +506,6 @@ int pme_eval_host(pme_recip* h, const double* recip, const void* xyzq_host, int 
       return fail(PME_ENOMEM, "device allocation of the force buffer failed");
     }
     h->force_bytes = bytes;
-  }
-  if (h->accum_dirty) {
-    cudaError_t e = cudaMemsetAsync(h->st.accum, 0, h->st.G() * 8, h->stream);
-    if (e != cudaSuccess) return cuda_fail(e, "eval_host: clear grid");
-    h->accum_dirty = false;
   }
   if (int rc = ensure_bins(h, ncoord)) return rc;
   const int ev = (calc_energy || calc_virial) ? 1 : 0;
@@ -579,7 +578,6 @@ int pme_load_charge_grid(pme_recip* h, const float* host_in) {
   cudaError_t e = cudaStreamSynchronize(h->stream);
   if (e == cudaSuccess) e = cudaMemcpy(h->st.accum, tmp.data(), tmp.size() * 8, cudaMemcpyHostToDevice);
   if (e != cudaSuccess) return cuda_fail(e, "load_charge_grid");
-  h->accum_dirty = true;
   return PME_OK;
 }
 
@@ -594,7 +592,7 @@ int pme_get_status(pme_recip* h, int* device_status) {
   if (status != kStatusOk) {
     // clear the sticky status, the barrier words, the accumulation grid and the accumulators
     // (an interrupted evaluation leaves them partly filled) so the handle is usable again
-    e = cudaMemsetAsync(h->d_bar, 0, 4 * sizeof(unsigned long long), h->stream);
+    e = cudaMemsetAsync(h->d_bar, 0, kBarWords * sizeof(unsigned long long), h->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(h->st.accum, 0, h->st.G() * 8, h->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(h->st.acc, 0, kAccCount * sizeof(long long), h->stream);
     if (e == cudaSuccess && h->d_bins)
@@ -953,11 +951,6 @@ int pme_autotune(pme_recip* h, const void* xyzq, int ncoord, double inv_boxx, do
   if (reps < 1 || reps > 100000) return fail(PME_EINVAL, "reps must be in [1, 100000]");
   DeviceGuard dg(h->device);
   cudaError_t e = cudaSuccess;
-  if (h->accum_dirty) {
-    e = cudaMemsetAsync(h->st.accum, 0, h->st.G() * 8, h->stream);
-    if (e != cudaSuccess) return cuda_fail(e, "autotune: clear grid");
-    h->accum_dirty = false;
-  }
   if (int rc = ensure_bins(h, ncoord)) return rc;
   // scratch force output and the energy/virial record to put back afterwards
   const int stride = std::max(ncoord, 1);

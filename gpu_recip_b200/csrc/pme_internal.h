@@ -43,11 +43,42 @@ size_t fused_smem_bytes(const SysDesc& d);
 void fused_tile_counts(const SysDesc& d, int* counts);
 int fused_barriers(const int* total);
 
+// Phases of a staged cooperative launch (k_staged): one reference-interface call each.
+enum StagedKind {
+  kStgBin = 0, kStgSpreadRows, kStgXFwd, kStgYFwd, kStgZFwd, kStgKtab, kStgZSolve, kStgFinalizeSolve,
+  kStgZInv, kStgYInv, kStgXInv
+};
+constexpr int kStagedMaxPhases = 4;
+
+struct StagedArgs {
+  SysDesc d;
+  int nphase;
+  int kind[kStagedMaxPhases];
+  int total[kStagedMaxPhases];
+  unsigned long long* bar;   // the handle's barrier words (shared with its fused evaluations)
+  int* status;
+  unsigned int spin_limit;
+  int bins;                  // 1: the launch bins atoms and advances the bin parity
+};
+
+// The handle's barrier words and failure-detection settings for a staged launch.
+struct StagedCtx {
+  unsigned long long* bar;
+  int* status;
+  unsigned int spin_limit;
+};
+
+// Global-atomic spread of one tile per CTA into a cleared accumulation grid (no bins needed).
 cudaError_t staged_spread(const SysDesc& d, cudaStream_t s);
-cudaError_t staged_self(const SysDesc& d, cudaStream_t s);
-cudaError_t staged_r2c(const SysDesc& d, bool zero_accum, cudaStream_t s);
-cudaError_t staged_solve(const SysDesc& d, cudaStream_t s);
-cudaError_t staged_c2r(const SysDesc& d, cudaStream_t s);
+// Reference-interface calls as cooperative launches: bin + exact row-block spread into the int64
+// grid (every point written); x, y, z forward passes; influence tables, solve with energy/virial
+// and the record update; z, y, x inverse passes.
+cudaError_t staged_spread_binned(const SysDesc& d, const StagedCtx& c, cudaStream_t s);
+cudaError_t staged_r2c(const SysDesc& d, const StagedCtx& c, cudaStream_t s);
+cudaError_t staged_solve(const SysDesc& d, const StagedCtx& c, cudaStream_t s);
+cudaError_t staged_c2r(const SysDesc& d, const StagedCtx& c, cudaStream_t s);
+// Self energy in one launch (done: an arrival counter, zero between launches).
+cudaError_t staged_self(const SysDesc& d, unsigned int* done, cudaStream_t s);
 cudaError_t staged_gather(const SysDesc& d, cudaStream_t s);
 
 // Launch shape of a fused evaluation: which build of the kernel and how many CTAs.

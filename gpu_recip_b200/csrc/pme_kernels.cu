@@ -18,6 +18,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
+#include <cstring>
 #include <map>
 #include <mutex>
 #include <utility>
@@ -54,59 +56,10 @@ __global__ void __launch_bounds__(kThreads) k_spread(const __grid_constant__ Sys
   spread_dispatch(d, blockIdx.x, smem);
 }
 
-__global__ void __launch_bounds__(kThreads) k_self(const __grid_constant__ SysDesc p) {
-  __shared__ SysDesc d;
-  __shared__ long long red[32];
-  load_desc(d, p);
-  long long q2 = 0;
-  for (int i = blockIdx.x * kThreads + threadIdx.x; i < d.natom; i += gridDim.x * kThreads)
-    q2 += q2_fixed(__ldg(&d.xyzq[i]).w);
-  const long long sum = block_sum_ll(q2, red);
-  if (threadIdx.x == 0 && sum != 0) atomicAdd((unsigned long long*)&d.acc[kAccQ2], (unsigned long long)sum);
-}
-
-__global__ void __launch_bounds__(kThreads) k_ktab(const __grid_constant__ SysDesc p) {
-  __shared__ SysDesc d;
-  load_desc(d, p);
-  ktab_tile(d);
-}
-
-__global__ void __launch_bounds__(kThreads) k_x_fwd(const __grid_constant__ SysDesc p, int zero_accum) {
-  __shared__ SysDesc d;
-  extern __shared__ float2 smem[];
-  load_desc(d, p);
-  x_fwd_tile(d, blockIdx.x, smem, zero_accum != 0);
-}
-
-__global__ void __launch_bounds__(kThreads) k_x_inv(const __grid_constant__ SysDesc p) {
-  __shared__ SysDesc d;
-  extern __shared__ float2 smem[];
-  load_desc(d, p);
-  x_inv_tile(d, blockIdx.x, smem);
-}
-
-__global__ void __launch_bounds__(kThreads) k_ypass(const __grid_constant__ SysDesc p, int mode) {
-  __shared__ SysDesc d;
-  extern __shared__ float2 smem[];
-  load_desc(d, p);
-  y_tile(d, mode, blockIdx.x, smem);
-}
-
-__global__ void __launch_bounds__(kThreads) k_zpass(const __grid_constant__ SysDesc p, int mode) {
-  __shared__ SysDesc d;
-  extern __shared__ float2 smem[];
-  load_desc(d, p);
-  z_tile(d, mode, blockIdx.x, smem);
-}
-
 __global__ void __launch_bounds__(kThreads) k_gather(const __grid_constant__ SysDesc p) {
   __shared__ SysDesc d;
   load_desc(d, p);
   gather_dispatch(d, blockIdx.x);
-}
-
-__global__ void k_finalize(const __grid_constant__ SysDesc p, int solve, int self) {
-  if (threadIdx.x == 0 && blockIdx.x == 0) finalize_system(p, solve != 0, self != 0);
 }
 
 // ------------------------------- fused persistent kernel --------------------------------------
@@ -155,7 +108,7 @@ __device__ __forceinline__ void red_release_add_u64(unsigned long long* p, unsig
 // when every CTA has read it).  Waits are bounded: after spin_limit polls the CTA records
 // kStatusBarrierTimeout in *status and the kernel returns (no trap, no hang).
 __device__ bool grid_barrier(unsigned long long* bar, unsigned long long base, int k, int nbar,
-                             int* status, unsigned int spin_limit) {
+                             int* status, unsigned int spin_limit, bool bump_parity = true) {
   __shared__ int ok;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -177,7 +130,9 @@ __device__ bool grid_barrier(unsigned long long* bar, unsigned long long base, i
     fence_acq_rel_gpu();
     if (good && k == 0 && blockIdx.x == 0) {
       bar[1] = base + (unsigned long long)nbar * gridDim.x;
-      bar[3] = bar[3] + 1ull;   // launch counter (bin parity); every CTA read it before barrier 0
+      // launch counter (bin parity), advanced by the launches that bin atoms; every CTA read it
+      // before barrier 0
+      if (bump_parity) bar[3] = bar[3] + 1ull;
     }
     ok = good;
   }
@@ -275,6 +230,67 @@ __device__ __forceinline__ void fused_body(const FusedArgs& a) {
 __global__ void __launch_bounds__(kThreads) k_fused_lat(const __grid_constant__ FusedArgs a) { fused_body<true>(a); }
 __global__ void __launch_bounds__(kThreads, 3) k_fused_tput(const __grid_constant__ FusedArgs a) { fused_body<false>(a); }
 
+// ------------------------------- staged cooperative kernel -----------------------------------
+// One reference-interface call (spread_charge, r2c_fft, scalar_sum, c2r_fft) as one cooperative
+// launch over the same tile functions as the fused evaluation, with bounded grid barriers between
+// its phases: fewer launches and no memset, the same arithmetic (so the same bits).
+__global__ void __launch_bounds__(kThreads, 2) k_staged(const __grid_constant__ StagedArgs a) {
+  __shared__ SysDesc d;
+  extern __shared__ float2 smem[];
+  __shared__ unsigned long long base;
+  __shared__ int parity;
+  if (threadIdx.x == 0) {
+    base = ld_acquire_u64(&a.bar[1]);
+    parity = (int)(ld_acquire_u64(&a.bar[3]) & 1ull);
+  }
+  if (ld_volatile(a.status) != kStatusOk) return;
+  load_desc(d, a.d);
+  const int nbar = a.nphase - 1;
+  for (int ph = 0; ph < a.nphase; ph++) {
+    for (int t = blockIdx.x; t < a.total[ph]; t += gridDim.x) {
+      switch (a.kind[ph]) {
+        case kStgBin: bin_tile(d, t, parity, (long long*)smem); break;
+        case kStgSpreadRows: spread_rows_dispatch(d, t, parity, (char*)smem); break;
+        case kStgXFwd: x_fwd_tile(d, t, smem, false); break;
+        case kStgYFwd: y_tile(d, 0, t, smem); break;
+        case kStgZFwd: z_tile(d, 0, t, smem); break;
+        case kStgKtab: ktab_tile(d); break;
+        case kStgZSolve: z_tile(d, 3, t, smem); break;
+        case kStgFinalizeSolve:
+          if (threadIdx.x == 0) finalize_system(d, true, false);
+          break;
+        case kStgZInv: z_tile(d, 1, t, smem); break;
+        case kStgYInv: y_tile(d, 1, t, smem); break;
+        default: x_inv_tile(d, t, smem); break;
+      }
+      __syncthreads();
+    }
+    if (ph < nbar && !grid_barrier(a.bar, base, ph, nbar, a.status, a.spin_limit, a.bins != 0)) return;
+  }
+}
+
+// Self energy in one launch: per-CTA sums of q^2 (fixed point) into the accumulator; the last CTA
+// to finish (ticket of an arrival counter) converts it into the record and re-arms the counter.
+__global__ void __launch_bounds__(kThreads) k_self_energy(const __grid_constant__ SysDesc p, unsigned int* done) {
+  __shared__ long long red[32];
+  __shared__ bool last;
+  long long q2 = 0;
+  for (int i = blockIdx.x * kThreads + threadIdx.x; i < p.natom; i += gridDim.x * kThreads)
+    q2 += q2_fixed(__ldg(&p.xyzq[i]).w);
+  const long long sum = block_sum_ll(q2, red);
+  if (threadIdx.x == 0) {
+    if (sum != 0) atomicAdd((unsigned long long*)&p.acc[kAccQ2], (unsigned long long)sum);
+    __threadfence();
+    last = atomicAdd(done, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    __threadfence();
+    finalize_system(p, false, true);
+    *done = 0u;
+  }
+}
+
 // ------------------------------- host launchers ----------------------------------------------
 static size_t staged_fft_smem(int L, int tx) { return tile_smem_bytes(L, tx) + 32 * 7 * sizeof(long long); }
 // z tiles also stage the y and z influence tables
@@ -326,44 +342,94 @@ cudaError_t staged_spread(const SysDesc& d, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-cudaError_t staged_self(const SysDesc& d, cudaStream_t s) {
-  int blocks = (d.natom + kThreads - 1) / kThreads;
-  blocks = blocks < 1 ? 1 : (blocks > 1024 ? 1024 : blocks);
-  k_self<<<blocks, kThreads, 0, s>>>(d);
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
-  k_finalize<<<1, 32, 0, s>>>(d, 0, 1);
+cudaError_t staged_self(const SysDesc& d, unsigned int* done, cudaStream_t s) {
+  int blocks = (d.natom + 4 * kThreads - 1) / (4 * kThreads);
+  blocks = blocks < 1 ? 1 : (blocks > 592 ? 592 : blocks);
+  k_self_energy<<<blocks, kThreads, 0, s>>>(d, done);
   return cudaGetLastError();
 }
 
-cudaError_t staged_r2c(const SysDesc& d, bool zero_accum, cudaStream_t s) {
-  k_x_fwd<<<tiles_xpass(d), kThreads, staged_fft_smem(d.g.nx, d.tx_rows), s>>>(d, zero_accum ? 1 : 0);
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
-  k_ypass<<<tiles_ypass(d), kThreads, staged_fft_smem(d.g.ny, d.tx_y), s>>>(d, 0);
-  if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  k_zpass<<<tiles_zpass(d), kThreads, staged_z_smem(d), s>>>(d, 0);
-  return cudaGetLastError();
+// Shared memory of a staged phase.
+static size_t staged_phase_smem(const SysDesc& d, int kind) {
+  switch (kind) {
+    case kStgBin: return 32 * sizeof(long long);
+    case kStgSpreadRows: return spread_x_smem_bytes(d.g.nx, d.bry * d.brz, d.order);
+    case kStgXFwd: case kStgXInv: return staged_fft_smem(d.g.nx, d.tx_rows);
+    case kStgYFwd: case kStgYInv: return staged_fft_smem(d.g.ny, d.tx_y);
+    case kStgZFwd: case kStgZSolve: case kStgZInv: return staged_z_smem(d);
+    default: return 0;
+  }
 }
 
-cudaError_t staged_solve(const SysDesc& d, cudaStream_t s) {
-  k_ktab<<<1, kThreads, 0, s>>>(d);
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
-  k_zpass<<<tiles_zpass(d), kThreads, staged_z_smem(d), s>>>(d, 3);
-  if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  k_finalize<<<1, 32, 0, s>>>(d, 1, 0);
-  return cudaGetLastError();
+static int staged_phase_tiles(const SysDesc& d, int kind) {
+  switch (kind) {
+    case kStgBin: return tiles_bin(d);
+    case kStgSpreadRows: return tiles_blocks(d);
+    case kStgXFwd: case kStgXInv: return tiles_xpass(d);
+    case kStgYFwd: case kStgYInv: return tiles_ypass(d);
+    case kStgZFwd: case kStgZSolve: case kStgZInv: return tiles_zpass(d);
+    default: return 1;   // kStgKtab, kStgFinalizeSolve
+  }
 }
 
-cudaError_t staged_c2r(const SysDesc& d, cudaStream_t s) {
-  k_zpass<<<tiles_zpass(d), kThreads, staged_z_smem(d), s>>>(d, 1);
-  cudaError_t e = cudaGetLastError();
+cudaError_t staged_launch(const SysDesc& d, const int* kinds, int nphase, const StagedCtx& c, cudaStream_t s) {
+  static std::mutex mu;
+  static std::map<std::pair<int, size_t>, int> occ_cache;
+  StagedArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.d = d;
+  a.nphase = nphase;
+  a.bar = c.bar;
+  a.status = c.status;
+  a.spin_limit = c.spin_limit;
+  size_t smem = 32 * sizeof(long long);
+  int most = 1;
+  for (int p = 0; p < nphase; p++) {
+    a.kind[p] = kinds[p];
+    a.total[p] = staged_phase_tiles(d, kinds[p]);
+    if (kinds[p] == kStgBin) a.bins = 1;
+    smem = std::max(smem, staged_phase_smem(d, kinds[p]));
+    most = std::max(most, a.total[p]);
+  }
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
-  k_ypass<<<tiles_ypass(d), kThreads, staged_fft_smem(d.g.ny, d.tx_y), s>>>(d, 1);
-  if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  k_x_inv<<<tiles_xpass(d), kThreads, staged_fft_smem(d.g.nx, d.tx_rows), s>>>(d);
-  return cudaGetLastError();
+  int occ = 0, sms = 0;
+  {
+    std::lock_guard<std::mutex> g(mu);
+    auto it = occ_cache.find({dev, smem});
+    if (it != occ_cache.end()) occ = it->second;
+  }
+  if (occ == 0) {
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_staged, kThreads, smem)) != cudaSuccess) return e;
+    if (occ < 1) return cudaErrorInvalidConfiguration;
+    std::lock_guard<std::mutex> g(mu);
+    occ_cache[{dev, smem}] = occ;
+  }
+  if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+  const int grid = std::min(sms * occ, most);
+  void* params[] = {&a};
+  return cudaLaunchCooperativeKernel((const void*)k_staged, dim3(grid), dim3(kThreads), params, smem, s);
+}
+
+cudaError_t staged_spread_binned(const SysDesc& d, const StagedCtx& c, cudaStream_t s) {
+  const int kinds[2] = {kStgBin, kStgSpreadRows};
+  return staged_launch(d, kinds, 2, c, s);
+}
+
+cudaError_t staged_r2c(const SysDesc& d, const StagedCtx& c, cudaStream_t s) {
+  const int kinds[3] = {kStgXFwd, kStgYFwd, kStgZFwd};
+  return staged_launch(d, kinds, 3, c, s);
+}
+
+cudaError_t staged_solve(const SysDesc& d, const StagedCtx& c, cudaStream_t s) {
+  const int kinds[3] = {kStgKtab, kStgZSolve, kStgFinalizeSolve};
+  return staged_launch(d, kinds, 3, c, s);
+}
+
+cudaError_t staged_c2r(const SysDesc& d, const StagedCtx& c, cudaStream_t s) {
+  const int kinds[3] = {kStgZInv, kStgYInv, kStgXInv};
+  return staged_launch(d, kinds, 3, c, s);
 }
 
 cudaError_t staged_gather(const SysDesc& d, cudaStream_t s) {
@@ -450,12 +516,9 @@ cudaError_t configure_kernels(size_t* max_dyn_smem) {
   e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   if (e != cudaSuccess) return e;
   if ((e = opt_in_smem(k_spread, optin)) != cudaSuccess) return e;
-  if ((e = opt_in_smem(k_x_fwd, optin)) != cudaSuccess) return e;
-  if ((e = opt_in_smem(k_x_inv, optin)) != cudaSuccess) return e;
-  if ((e = opt_in_smem(k_ypass, optin)) != cudaSuccess) return e;
-  if ((e = opt_in_smem(k_zpass, optin)) != cudaSuccess) return e;
   if ((e = opt_in_smem(k_fused_lat, optin)) != cudaSuccess) return e;
   if ((e = opt_in_smem(k_fused_tput, optin)) != cudaSuccess) return e;
+  if ((e = opt_in_smem(k_staged, optin)) != cudaSuccess) return e;
   cudaFuncAttributes fa;
   if ((e = cudaFuncGetAttributes(&fa, k_fused_lat)) != cudaSuccess) return e;
   if (max_dyn_smem) *max_dyn_smem = (size_t)optin - fa.sharedSizeBytes;
