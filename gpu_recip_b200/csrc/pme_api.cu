@@ -54,6 +54,7 @@ struct pme_recip {
   int plane_mode = 0;   // 0 automatic, 1 whole-plane tiles where they fit, 2 separate passes
   int grid_cap = 0;     // CTAs of the persistent launch (0: as many as are resident)
   int x_gather = PME_XGATHER_AUTO;   // PME_XGATHER_*
+  bool accum_zero = true;    // the int64 charge grid is known to be all zero (staged spread skips its clear)
   float* d_force = nullptr;      // pme_eval_host: device forces before the copy to the host
   size_t force_bytes = 0;
 };
@@ -329,13 +330,14 @@ int pme_spread_charge(pme_recip* h, const void* xyzq, int ncoord, const double* 
   if (ncoord < 0 || (ncoord > 0 && !xyzq)) return fail(PME_EINVAL, "bad xyzq/ncoord");
   if (int rc = check_recip(recip)) return rc;
   DeviceGuard dg(h->device);
-  if (int rc = ensure_bins(h, ncoord)) return rc;
-  // bin by row block, then each block's exact rows to the int64 grid (every point is written)
-  SysDesc d = h->st.desc9(recip, 0.0, xyzq, ncoord, nullptr, 0, 0, 0, 0);
-  int sms = 148;
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
-  d.bin_atoms = (ncoord + kThreads - 1) / kThreads < sms ? kThreads / 2 : kThreads;
-  cudaError_t e = staged_spread_binned(d, staged_ctx(h), h->stream);
+  // the atomic spread adds into the int64 grid: clear it unless it is known to be zero (after
+  // creation and after r2c_fft, which clears it behind its read)
+  if (!h->accum_zero) {
+    cudaError_t e = cudaMemsetAsync(h->st.accum, 0, h->st.G() * 8, h->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "spread_charge: clear grid");
+  }
+  h->accum_zero = false;
+  cudaError_t e = staged_spread(h->st.desc9(recip, 0.0, xyzq, ncoord, nullptr, 0, 0, 0, 0), h->stream);
   if (e != cudaSuccess) return cuda_fail(e, "spread_charge");
   return PME_OK;
 }
@@ -345,6 +347,7 @@ int pme_r2c_fft(pme_recip* h) {
   DeviceGuard dg(h->device);
   cudaError_t e = staged_r2c(h->st.desc(nullptr, 0.0, nullptr, 0, nullptr, 0, 0, 0, 0), staged_ctx(h), h->stream);
   if (e != cudaSuccess) return cuda_fail(e, "r2c_fft");
+  h->accum_zero = true;
   return PME_OK;
 }
 
@@ -578,6 +581,7 @@ int pme_load_charge_grid(pme_recip* h, const float* host_in) {
   cudaError_t e = cudaStreamSynchronize(h->stream);
   if (e == cudaSuccess) e = cudaMemcpy(h->st.accum, tmp.data(), tmp.size() * 8, cudaMemcpyHostToDevice);
   if (e != cudaSuccess) return cuda_fail(e, "load_charge_grid");
+  h->accum_zero = false;
   return PME_OK;
 }
 
@@ -599,6 +603,7 @@ int pme_get_status(pme_recip* h, int* device_status) {
       e = cudaMemsetAsync(h->d_bins, 0, h->st.bin_ints(h->st.atom_cap) * sizeof(int), h->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) return cuda_fail(e, "get_status: reset");
+    h->accum_zero = true;
     return fail(PME_ETIMEOUT, "a grid barrier of the fused evaluation timed out");
   }
   return PME_OK;

@@ -44,9 +44,10 @@ void fused_tile_counts(const SysDesc& d, int* counts);
 int fused_barriers(const int* total);
 
 // Phases of a staged cooperative launch (k_staged): one reference-interface call each.
+// kStgXFwdZero reads the int64 charge grid and leaves it zero behind it (ready for the next
+// atomic spread).
 enum StagedKind {
-  kStgBin = 0, kStgSpreadRows, kStgXFwd, kStgYFwd, kStgZFwd, kStgKtab, kStgZSolve, kStgFinalizeSolve,
-  kStgZInv, kStgYInv, kStgXInv
+  kStgXFwdZero = 0, kStgYFwd, kStgZFwd, kStgKtab, kStgZSolve, kStgFinalizeSolve, kStgZInv, kStgYInv, kStgXInv
 };
 constexpr int kStagedMaxPhases = 4;
 
@@ -58,7 +59,6 @@ struct StagedArgs {
   unsigned long long* bar;   // the handle's barrier words (shared with its fused evaluations)
   int* status;
   unsigned int spin_limit;
-  int bins;                  // 1: the launch bins atoms and advances the bin parity
 };
 
 // The handle's barrier words and failure-detection settings for a staged launch.
@@ -68,12 +68,11 @@ struct StagedCtx {
   unsigned int spin_limit;
 };
 
-// Global-atomic spread of one tile per CTA into a cleared accumulation grid (no bins needed).
+// Global-atomic spread of one tile per CTA into a cleared accumulation grid (exact int64 sums).
 cudaError_t staged_spread(const SysDesc& d, cudaStream_t s);
-// Reference-interface calls as cooperative launches: bin + exact row-block spread into the int64
-// grid (every point written); x, y, z forward passes; influence tables, solve with energy/virial
-// and the record update; z, y, x inverse passes.
-cudaError_t staged_spread_binned(const SysDesc& d, const StagedCtx& c, cudaStream_t s);
+// Reference-interface calls as cooperative launches: x (clearing the charge grid behind it), y, z
+// forward passes; influence tables, solve with energy/virial and the record update; z, y, x
+// inverse passes.
 cudaError_t staged_r2c(const SysDesc& d, const StagedCtx& c, cudaStream_t s);
 cudaError_t staged_solve(const SysDesc& d, const StagedCtx& c, cudaStream_t s);
 cudaError_t staged_c2r(const SysDesc& d, const StagedCtx& c, cudaStream_t s);

@@ -231,27 +231,22 @@ __global__ void __launch_bounds__(kThreads) k_fused_lat(const __grid_constant__ 
 __global__ void __launch_bounds__(kThreads, 3) k_fused_tput(const __grid_constant__ FusedArgs a) { fused_body<false>(a); }
 
 // ------------------------------- staged cooperative kernel -----------------------------------
-// One reference-interface call (spread_charge, r2c_fft, scalar_sum, c2r_fft) as one cooperative
-// launch over the same tile functions as the fused evaluation, with bounded grid barriers between
-// its phases: fewer launches and no memset, the same arithmetic (so the same bits).
+// One reference-interface call (r2c_fft, scalar_sum, c2r_fft) as one cooperative launch over the
+// same tile functions as the fused evaluation, with bounded grid barriers between its phases:
+// one launch per call instead of three, the same arithmetic (so the same bits).  The launches do
+// not bin atoms, so they leave the bin parity of the fused evaluations alone.
 __global__ void __launch_bounds__(kThreads, 2) k_staged(const __grid_constant__ StagedArgs a) {
   __shared__ SysDesc d;
   extern __shared__ float2 smem[];
   __shared__ unsigned long long base;
-  __shared__ int parity;
-  if (threadIdx.x == 0) {
-    base = ld_acquire_u64(&a.bar[1]);
-    parity = (int)(ld_acquire_u64(&a.bar[3]) & 1ull);
-  }
+  if (threadIdx.x == 0) base = ld_acquire_u64(&a.bar[1]);
   if (ld_volatile(a.status) != kStatusOk) return;
   load_desc(d, a.d);
   const int nbar = a.nphase - 1;
   for (int ph = 0; ph < a.nphase; ph++) {
     for (int t = blockIdx.x; t < a.total[ph]; t += gridDim.x) {
       switch (a.kind[ph]) {
-        case kStgBin: bin_tile(d, t, parity, (long long*)smem); break;
-        case kStgSpreadRows: spread_rows_dispatch(d, t, parity, (char*)smem); break;
-        case kStgXFwd: x_fwd_tile(d, t, smem, false); break;
+        case kStgXFwdZero: x_fwd_tile(d, t, smem, true); break;
         case kStgYFwd: y_tile(d, 0, t, smem); break;
         case kStgZFwd: z_tile(d, 0, t, smem); break;
         case kStgKtab: ktab_tile(d); break;
@@ -265,7 +260,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_staged(const __grid_constant__ 
       }
       __syncthreads();
     }
-    if (ph < nbar && !grid_barrier(a.bar, base, ph, nbar, a.status, a.spin_limit, a.bins != 0)) return;
+    if (ph < nbar && !grid_barrier(a.bar, base, ph, nbar, a.status, a.spin_limit, false)) return;
   }
 }
 
@@ -352,9 +347,7 @@ cudaError_t staged_self(const SysDesc& d, unsigned int* done, cudaStream_t s) {
 // Shared memory of a staged phase.
 static size_t staged_phase_smem(const SysDesc& d, int kind) {
   switch (kind) {
-    case kStgBin: return 32 * sizeof(long long);
-    case kStgSpreadRows: return spread_x_smem_bytes(d.g.nx, d.bry * d.brz, d.order);
-    case kStgXFwd: case kStgXInv: return staged_fft_smem(d.g.nx, d.tx_rows);
+    case kStgXFwdZero: case kStgXInv: return staged_fft_smem(d.g.nx, d.tx_rows);
     case kStgYFwd: case kStgYInv: return staged_fft_smem(d.g.ny, d.tx_y);
     case kStgZFwd: case kStgZSolve: case kStgZInv: return staged_z_smem(d);
     default: return 0;
@@ -363,9 +356,7 @@ static size_t staged_phase_smem(const SysDesc& d, int kind) {
 
 static int staged_phase_tiles(const SysDesc& d, int kind) {
   switch (kind) {
-    case kStgBin: return tiles_bin(d);
-    case kStgSpreadRows: return tiles_blocks(d);
-    case kStgXFwd: case kStgXInv: return tiles_xpass(d);
+    case kStgXFwdZero: case kStgXInv: return tiles_xpass(d);
     case kStgYFwd: case kStgYInv: return tiles_ypass(d);
     case kStgZFwd: case kStgZSolve: case kStgZInv: return tiles_zpass(d);
     default: return 1;   // kStgKtab, kStgFinalizeSolve
@@ -387,7 +378,6 @@ cudaError_t staged_launch(const SysDesc& d, const int* kinds, int nphase, const 
   for (int p = 0; p < nphase; p++) {
     a.kind[p] = kinds[p];
     a.total[p] = staged_phase_tiles(d, kinds[p]);
-    if (kinds[p] == kStgBin) a.bins = 1;
     smem = std::max(smem, staged_phase_smem(d, kinds[p]));
     most = std::max(most, a.total[p]);
   }
@@ -412,13 +402,8 @@ cudaError_t staged_launch(const SysDesc& d, const int* kinds, int nphase, const 
   return cudaLaunchCooperativeKernel((const void*)k_staged, dim3(grid), dim3(kThreads), params, smem, s);
 }
 
-cudaError_t staged_spread_binned(const SysDesc& d, const StagedCtx& c, cudaStream_t s) {
-  const int kinds[2] = {kStgBin, kStgSpreadRows};
-  return staged_launch(d, kinds, 2, c, s);
-}
-
 cudaError_t staged_r2c(const SysDesc& d, const StagedCtx& c, cudaStream_t s) {
-  const int kinds[3] = {kStgXFwd, kStgYFwd, kStgZFwd};
+  const int kinds[3] = {kStgXFwdZero, kStgYFwd, kStgZFwd};
   return staged_launch(d, kinds, 3, c, s);
 }
 

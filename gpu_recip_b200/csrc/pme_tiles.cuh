@@ -971,10 +971,7 @@ __device__ __forceinline__ void spread_items(const SpreadLists& sl, int nitems, 
   }
 }
 
-// TO_ACCUM (the staged spread_charge): after spreading, the block's exact int64 rows are stored
-// to the accumulation grid d.accum ([z][y][x]) instead of being converted and x-transformed.
-// Every row block writes all of its points, so the grid needs no clearing beforehand.
-template <int P, bool TO_ACCUM = false>
+template <int P>
 __device__ __forceinline__ void spread_x_tile(const SysDesc& d, int tile, int parity, char* smem_raw) {
   constexpr int RF = rec_floats(P);
   constexpr int NW4 = (RF - 8) / 4;          // float4s of spreading weights
@@ -1113,22 +1110,6 @@ __device__ __forceinline__ void spread_x_tile(const SysDesc& d, int tile, int pa
     if (tid < 2) d.bin_meta[2 * tid + 1 - parity] = 0;   // overflow count, max |q|
   }
   const int sh = mode == kSplit2 ? k2 : 32;
-  if (TO_ACCUM) {
-    const FastDiv nryd0 = make_fastdiv(nry);
-    for (int idx = tid; idx < nry * nrz * L; idx += kThreads) {
-      const int t = fdiv(idx, plan.n_div), e = idx - t * L;
-      const int a = t * Lp + e;
-      unsigned long long u = (unsigned long long)s0[a] + ((unsigned long long)s1[a] << 16) +
-                             ((unsigned long long)(long long)s2[a] << sh);
-      if (e < P - 1)
-        u += (unsigned long long)s0[a + L] + ((unsigned long long)s1[a + L] << 16) +
-             ((unsigned long long)(long long)s2[a + L] << sh);
-      const int rz = fdiv(t, nryd0), ry = t - rz * nry;
-      __stcg(&d.accum[((size_t)(Z0 + rz) * g.ny + (Y0 + ry)) * L + e], u);
-    }
-    __syncthreads();
-    return;
-  }
   if (tid < L) tw[tid] = tw0;
   if (tid + kThreads < L) tw[tid + kThreads] = tw1;
   // rows: r = ry + nry*rz (r < nry*nrz valid); FFT line t = r.  Point e of a row also takes the
@@ -1160,15 +1141,6 @@ __device__ __forceinline__ void spread_x_tile(const SysDesc& d, int tile, int pa
   }
   __syncthreads();
   step_mark(d, 6);
-}
-
-// The staged spread_charge's row-block tile: exact rows stored to the int64 accumulation grid.
-__device__ __forceinline__ void spread_rows_dispatch(const SysDesc& d, int tile, int parity, char* smem) {
-  switch (d.order) {
-    case 4: spread_x_tile<4, true>(d, tile, parity, smem); break;
-    case 6: spread_x_tile<6, true>(d, tile, parity, smem); break;
-    default: spread_x_tile<8, true>(d, tile, parity, smem); break;
-  }
 }
 
 __device__ __forceinline__ void spread_x_dispatch(const SysDesc& d, int tile, int parity, char* smem) {
