@@ -35,6 +35,8 @@ SIGNATURES = {
     "pme_create": [_I, _I, _I, _I, _I, _I, _I, _P, ctypes.POINTER(_P)],
     "pme_destroy": [_P],
     "pme_set_stream": [_P, _P],
+    "pme_get_stream": [_P, ctypes.POINTER(_P)],
+    "pme_recip_loop_run": [_P, _D, _P, ctypes.POINTER(ctypes.c_longlong)],
     "pme_set_order": [_P, _I],
     "pme_get_nfft": [_P, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I)],
     "pme_get_order": [_P, ctypes.POINTER(_I)],
@@ -123,6 +125,23 @@ class SystemDesc(ctypes.Structure):
                 ("box", ctypes.c_double * 3), ("kappa", ctypes.c_double), ("xyzq", _P),
                 ("force", _P), ("force_kind", _I), ("stride", _I), ("calc_energy", _I),
                 ("calc_virial", _I)]
+
+
+class RecipHeader(ctypes.Structure):
+    """pme_recip_header of include/pme_recip.h."""
+    _fields_ = [("inv_boxx", ctypes.c_double), ("inv_boxy", ctypes.c_double), ("inv_boxz", ctypes.c_double),
+                ("ncoord", _I), ("calc_energy", _I), ("calc_virial", _I)]
+
+
+RECV_HEADER = ctypes.CFUNCTYPE(_I, _P, ctypes.POINTER(RecipHeader))
+RECV_COORD = ctypes.CFUNCTYPE(_I, _P, _I, _P, ctypes.POINTER(_P))
+SEND_FORCE = ctypes.CFUNCTYPE(_I, _P, _I, _P, ctypes.POINTER(ctypes.c_double))
+
+
+class RecipComm(ctypes.Structure):
+    """pme_recip_comm of include/pme_recip.h."""
+    _fields_ = [("user", _P), ("recv_header", RECV_HEADER), ("recv_coord", RECV_COORD),
+                ("send_force", SEND_FORCE)]
 
 
 class TuneConfig(ctypes.Structure):

@@ -283,6 +283,12 @@ int pme_set_stream(pme_recip* h, void* stream) {
   return PME_OK;
 }
 
+int pme_get_stream(const pme_recip* h, void** stream) {
+  if (!h || !stream) return fail(PME_EINVAL, "NULL argument");
+  *stream = (void*)h->stream;
+  return PME_OK;
+}
+
 int pme_set_order(pme_recip* h, int order) {
   if (int rc = handle_ok(h)) return rc;
   if (int rc = check_grid(h->st.nx, h->st.ny, h->st.nz, order)) return rc;
@@ -821,10 +827,8 @@ int pme_batch_eval(pme_batch* b) {
 int pme_batch_clear_energy_virial(pme_batch* b) {
   if (!b) return fail(PME_EINVAL, "batch is NULL");
   DeviceGuard dg(b->device);
-  for (size_t i = 0; i < b->st.size(); i++) {
-    cudaError_t e = cudaMemsetAsync(b->st[i].ev, 0, kEvCount * sizeof(double), b->stream);
-    if (e != cudaSuccess) return cuda_fail(e, "batch clear");
-  }
+  cudaError_t e = clear_records(b->d_desc, (int)b->desc.size(), b->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "batch clear");
   return PME_OK;
 }
 

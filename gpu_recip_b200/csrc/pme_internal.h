@@ -79,6 +79,8 @@ cudaError_t staged_c2r(const SysDesc& d, const StagedCtx& c, cudaStream_t s);
 // Self energy in one launch (done: an arrival counter, zero between launches).
 cudaError_t staged_self(const SysDesc& d, unsigned int* done, cudaStream_t s);
 cudaError_t staged_gather(const SysDesc& d, cudaStream_t s);
+// Zero the energy/virial records of the nsys systems of a device descriptor table.
+cudaError_t clear_records(const SysDesc* d_table, int nsys, cudaStream_t s);
 
 // Launch shape of a fused evaluation: which build of the kernel and how many CTAs.
 enum { kFusedLatency = 0, kFusedThroughput = 1 };

@@ -286,6 +286,14 @@ __global__ void __launch_bounds__(kThreads) k_self_energy(const __grid_constant_
   }
 }
 
+// Energy/virial records of every system of a batch set to zero in one launch (a memset per
+// system would cost one operation each).
+__global__ void k_clear_records(const SysDesc* __restrict__ table, int nsys) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int sys = i / kEvCount, slot = i - sys * kEvCount;
+  if (sys < nsys) table[sys].ev[slot] = 0.0;
+}
+
 // ------------------------------- host launchers ----------------------------------------------
 static size_t staged_fft_smem(int L, int tx) { return tile_smem_bytes(L, tx) + 32 * 7 * sizeof(long long); }
 // z tiles also stage the y and z influence tables
@@ -415,6 +423,12 @@ cudaError_t staged_solve(const SysDesc& d, const StagedCtx& c, cudaStream_t s) {
 cudaError_t staged_c2r(const SysDesc& d, const StagedCtx& c, cudaStream_t s) {
   const int kinds[3] = {kStgZInv, kStgYInv, kStgXInv};
   return staged_launch(d, kinds, 3, c, s);
+}
+
+cudaError_t clear_records(const SysDesc* d_table, int nsys, cudaStream_t s) {
+  const int n = nsys * kEvCount;
+  k_clear_records<<<(n + 255) / 256, 256, 0, s>>>(d_table, nsys);
+  return cudaGetLastError();
 }
 
 cudaError_t staged_gather(const SysDesc& d, cudaStream_t s) {

@@ -10,6 +10,7 @@ same loop over CudaDomdecRecip (one fused evaluation per step).
 """
 from __future__ import annotations
 
+import ctypes
 import queue
 from dataclasses import dataclass
 from typing import Optional
@@ -110,3 +111,81 @@ class RecipLooper:
             self.comm.send_force(RecipReply(self._force[:n].clone(), rec))
             self.steps += 1
         return self.steps
+
+
+_CUDART = None
+
+
+def _cudart():
+    """The CUDA runtime library, for a device-to-device copy of the loop's force buffer."""
+    global _CUDART
+    if _CUDART is None:
+        import ctypes.util
+        for name in ("libcudart.so", "libcudart.so.12", ctypes.util.find_library("cudart"),
+                     "/usr/local/cuda/lib64/libcudart.so"):
+            if not name:
+                continue
+            try:
+                _CUDART = ctypes.CDLL(name)
+                break
+            except OSError:
+                continue
+        if _CUDART is None:
+            raise RuntimeError("the CUDA runtime library was not found")
+    return _CUDART
+
+
+class NativeRecipLooper:
+    """The same loop run by the library itself (pme_recip_loop_run, C++ behind the C ABI): its
+    three transport callbacks read headers and coordinates from an InProcessRecipComm and post
+    the replies to it, so a direct side written against the queue protocol talks to the native
+    loop unchanged.  Each reply carries a copy of the step's float3 forces and its own
+    energy/virial record."""
+
+    def __init__(self, comm: InProcessRecipComm, nfftx: int, nffty: int, nfftz: int, order: int,
+                 kappa: float, stream=None):
+        from . import _capi as C
+        from .pme import CudaPMERecip
+        self.comm = comm
+        self.kappa = float(kappa)
+        self.pme = CudaPMERecip(nfftx, nffty, nfftz, order, stream=stream)
+        self._coords = None
+        self.steps = 0
+
+        def recv_header(user, hdr):
+            try:
+                h = comm._to_recip.get(timeout=comm.timeout)
+            except Exception:
+                return 1
+            hdr.contents.inv_boxx, hdr.contents.inv_boxy, hdr.contents.inv_boxz = h.inv_boxx, h.inv_boxy, h.inv_boxz
+            hdr.contents.ncoord = h.ncoord
+            hdr.contents.calc_energy, hdr.contents.calc_virial = int(h.calc_energy), int(h.calc_virial)
+            return 0
+
+        def recv_coord(user, ncoord, stream_ptr, out):
+            try:
+                self._coords = comm.recv_coord()
+            except Exception:
+                return 1
+            out[0] = self._coords.data_ptr() if ncoord > 0 else None
+            return 0
+
+        def send_force(user, ncoord, force_ptr, ev):
+            import torch
+            f = torch.empty((max(ncoord, 0), 3), dtype=torch.float32, device=self._coords.device)
+            if ncoord > 0 and _cudart().cudaMemcpy(ctypes.c_void_p(f.data_ptr()), ctypes.c_void_p(force_ptr),
+                                                  ctypes.c_size_t(12 * ncoord), 3) != 0:   # device to device
+                return 1
+            comm.send_force(RecipReply(f, np.ctypeslib.as_array(ev, shape=(11,)).copy()))
+            return 0
+
+        self._cb = C.RecipComm(None, C.RECV_HEADER(recv_header), C.RECV_COORD(recv_coord), C.SEND_FORCE(send_force))
+
+    def run(self) -> int:
+        from . import _capi as C
+        n = ctypes.c_longlong(0)
+        C.check(C.load().pme_recip_loop_run(self.pme._h, self.kappa, ctypes.byref(self._cb), ctypes.byref(n)),
+                "pme_recip_loop_run")
+        self.steps = n.value
+        return self.steps
+

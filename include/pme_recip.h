@@ -63,6 +63,7 @@ PME_API int pme_destroy(pme_recip* h);
 
 /* ---- configuration (CudaPMERecip.h:176-178, :198-201) ---- */
 PME_API int pme_set_stream(pme_recip* h, void* stream);
+PME_API int pme_get_stream(const pme_recip* h, void** stream);     /* the handle's cudaStream_t */
 PME_API int pme_set_order(pme_recip* h, int order);                 /* recomputes the B-spline moduli */
 PME_API int pme_get_nfft(const pme_recip* h, int* nfftx, int* nffty, int* nfftz);
 PME_API int pme_get_order(const pme_recip* h, int* order);
@@ -144,6 +145,33 @@ PME_API int pme_force_convert(const long long* in, int in_stride, int ncoord, vo
  * (add_type) SoA rows at add + k add_stride. */
 PME_API int pme_force_convert_add(long long* inout, int stride, int ncoord, const void* add, int add_stride,
                                   int add_type, void* stream);
+
+/* ---- recip-node request loop (CudaDomdecRecipLooper::run, CudaDomdecRecipLooper.cu:3-36) ----
+ * The loop of a pure reciprocal-space node: receive a header (DomdecRecipComm.h:11-15), stop on
+ * a negative coordinate count, receive the coordinates, evaluate (pme_eval_ortho into a float3
+ * force buffer that grows with the count, as reallocate<float3> does), send the forces, repeat.
+ * The transport is the caller's, as callbacks (the role of CudaDomdecRecipComm); each returns 0
+ * on success, anything else ends the loop with PME_ESTATE. */
+typedef struct {
+  double inv_boxx, inv_boxy, inv_boxz;   /* inverse box edges (1/A) */
+  int ncoord;                            /* coordinates of this step; < 0: STOP */
+  int calc_energy, calc_virial;
+} pme_recip_header;
+
+typedef struct {
+  void* user;                            /* passed back to every callback */
+  int (*recv_header)(void* user, pme_recip_header* header);
+  /* The step's coordinates: *xyzq = a device float4[ncoord] (the callback may copy them there
+   * on `stream`, the handle's stream, which the evaluation then follows). */
+  int (*recv_coord)(void* user, int ncoord, void* stream, const void** xyzq);
+  /* After the step (stream synchronised): force = device float3[ncoord] (+dE/dx, overwritten by
+   * the next step), energy_virial = host double[PME_EV_COUNT], this step's own record. */
+  int (*send_force)(void* user, int ncoord, const void* force, const double* energy_virial);
+} pme_recip_comm;
+
+/* Runs the loop on the handle (its grid, order and stream) with Ewald kappa until STOP; *steps
+ * (may be NULL) receives the number of steps served.  Synchronous. */
+PME_API int pme_recip_loop_run(pme_recip* h, double kappa, const pme_recip_comm* comm, long long* steps);
 
 /* ---- grid read-back for parity checks (synchronise the stream; host outputs) ----
  * Layouts follow the reference: real grids [z][y][x]; half-complex grid [z][y][kx],

@@ -104,13 +104,16 @@ def test_force_convert_rejects_bad_arguments(cuda):
         force_convert(fi, 64, 32, out, 16)                  # output stride below ncoord
 
 
-def test_recip_looper_serves_a_direct_node(cuda):
+@pytest.mark.parametrize("native", [False, True])
+def test_recip_looper_serves_a_direct_node(cuda, native):
+    """The recip node's loop (CudaDomdecRecipLooper::run) in Python and in C++ behind the C ABI
+    (pme_recip_loop_run): every reply equals the MD adapter's own evaluation bit for bit."""
     torch = cuda
     from gpu_recip_b200 import CudaDomdecRecip
-    from gpu_recip_b200.looper import InProcessRecipComm, RecipLooper
+    from gpu_recip_b200.looper import InProcessRecipComm, NativeRecipLooper, RecipLooper
     s = S.config_small(seed=9)
     comm = InProcessRecipComm(timeout=120.0)
-    looper = RecipLooper(comm, *s.nfft, s.order, s.kappa)
+    looper = (NativeRecipLooper if native else RecipLooper)(comm, *s.nfft, s.order, s.kappa)
     out = {}
     th = threading.Thread(target=lambda: out.setdefault("steps", looper.run()))
     th.start()

@@ -24,7 +24,7 @@ def _build(tmp, name="recip_driver"):
     return exe
 
 
-@pytest.mark.parametrize("name", ["recip_driver", "direct_driver"])
+@pytest.mark.parametrize("name", ["recip_driver", "direct_driver", "looper_driver"])
 def test_cpp_driver_compiles_against_the_header(name):
     with tempfile.TemporaryDirectory() as tmp:
         obj = os.path.join(tmp, "d.o")
@@ -93,3 +93,47 @@ def test_cpp_direct_driver_on_reference_fixture(cuda):
     assert abs(main[0] - d["energy_vdw"]) < d["tol_energy"] and abs(main[1] - d["energy_elec"]) < d["tol_energy"]
     assert np.abs(main[3:12].reshape(3, 3) - d["virial"]).max() < d["tol_virial"]
     assert np.abs(total[12:].reshape(n, 3) - d["force_total"]).max() <= d["tol_force_total"]
+
+
+@pytest.mark.gpu
+def test_cpp_recip_node_loop(cuda):
+    """A C++ recip node on pme_recip_loop_run (CudaDomdecRecipLooper::run): three steps with
+    changing box, coordinate count and flags, then STOP; every step's forces and record equal the
+    MD adapter's evaluation of the same step bit for bit."""
+    torch = cuda
+    from gpu_recip_b200 import CudaDomdecRecip
+    from gpu_recip_b200 import systems as S
+    s = S.config_small(seed=12)
+    n = s.natom
+    with tempfile.TemporaryDirectory() as tmp:
+        exe = _build(tmp, "looper_driver")
+        inp, out = os.path.join(tmp, "in.bin"), os.path.join(tmp, "out.bin")
+        with open(inp, "wb") as fh:
+            fh.write(np.array([n, s.order, *s.nfft], np.int32).tobytes())
+            fh.write(np.asarray(s.box, np.float64).tobytes())
+            fh.write(np.array([s.kappa], np.float64).tobytes())
+            fh.write(np.ascontiguousarray(s.xyzq, np.float32).tobytes())
+        subprocess.run([exe, inp, out], check=True, timeout=120)
+        raw = open(out, "rb").read()
+    steps = int(np.frombuffer(raw[:8], np.int64)[0])
+    assert steps == 3
+    pos = 8
+    ref = CudaDomdecRecip(*s.nfft, s.order, s.kappa)
+    for k, (scale, drop, e, v) in enumerate([(1.0, 0, True, True), (1.01, 7, False, True), (0.995, 14, True, False)]):
+        cnt = int(np.frombuffer(raw[pos:pos + 4], np.int32)[0])
+        pos += 4
+        rec = np.frombuffer(raw[pos:pos + 88], np.float64)
+        pos += 88
+        force = np.frombuffer(raw[pos:pos + 12 * cnt], np.float32).reshape(cnt, 3)
+        pos += 12 * cnt
+        assert cnt == n - drop
+        x = torch.from_numpy(np.ascontiguousarray(s.xyzq[:cnt])).cuda()
+        want = torch.zeros((cnt, 3), dtype=torch.float32, device="cuda")
+        ev = ref.pme.energy_virial
+        ev.clear()
+        ref.calc(*[1.0 / (b * scale) for b in s.box], x, cnt, e, v, want)
+        torch.cuda.synchronize()
+        ev.copyToHost()
+        assert np.array_equal(force, want.cpu().numpy()), k
+        assert rec[0] == ev.getEnergy("recip") and np.array_equal(rec[2:].reshape(3, 3), ev.getVirial()), k
+
