@@ -167,6 +167,7 @@ int launch_fused_single(pme_recip* h, const SysDesc& d_in) {
     e = fused_shape(a.total, smem, h->grid_cap, &shape);
   }
   if (e != cudaSuccess) return cuda_fail(e, "fused: launch shape (does the kernel fit on an SM?)");
+  d.gsort = gather_sorts(d, smem);
   a.nbar = fused_barriers(a.total);
   a.single = d;
   e = fused_launch(a, shape, smem, h->stream);
@@ -780,6 +781,7 @@ int pme_batch_commit(pme_batch* b) {
     smem = std::max(smem, fused_smem_bytes(b->desc[i]));
   }
   for (int p = 0; p < kPhases; p++) b->total[p] = prefix[(size_t)p * (nsys + 1) + nsys];
+  for (int i = 0; i < nsys; i++) b->desc[i].gsort = gather_sorts(b->desc[i], smem);
   cudaError_t e = cudaStreamSynchronize(b->stream);
   if (e == cudaSuccess) e = cudaMemcpy(b->d_desc, b->desc.data(), sizeof(SysDesc) * nsys, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(b->d_prefix, prefix.data(), prefix.size() * sizeof(int), cudaMemcpyHostToDevice);

@@ -207,6 +207,9 @@ __device__ __forceinline__ void fused_body(const FusedArgs& a) {
             } else {
               gather_bin_order<true>(d, local, parity, (char*)smem);
             }
+          } else if (!LAT && d.gsort) {
+            // (throughput build only: large bins come with launches of many tiles per CTA)
+            gather_bin_order<false, true>(d, local, parity, (char*)smem);
           } else {
             gather_bin_order<false>(d, local, parity, (char*)smem);
           }

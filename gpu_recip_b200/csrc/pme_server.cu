@@ -389,6 +389,7 @@ int rebuild(pme_server* s) {
     sl.pad = 0;
   }
   for (int p = 0; p < kPhases; p++) s->total[p] = s->h_prefix[(size_t)p * (n + 1) + n];
+  for (int i = 0; i < n; i++) s->h_table[i].gsort = gather_sorts(s->h_table[i], s->smem);
   if (n == 0) return PME_OK;
   // Stream order puts these copies after the previous step's launches, which read the tables.
   // The pinned source alternates per rebuild; the copies from the buffer's previous use were
