@@ -114,7 +114,7 @@ _RESTYPES = {"pme_last_error_string": ctypes.c_char_p, "pme_status_string": ctyp
              "pme_system_device_bytes": ctypes.c_size_t, "pme_request_device_bytes": ctypes.c_size_t}
 
 PME_INJECT_NONE, PME_INJECT_SKIP_BARRIER = 0, 1
-PME_SCHED_AUTO, PME_SCHED_PLANES, PME_SCHED_PASSES = 0, 1, 2
+PME_SCHED_AUTO, PME_SCHED_PLANES, PME_SCHED_PASSES, PME_SCHED_CLUSTER = 0, 1, 2, 3
 PME_XGATHER_AUTO, PME_XGATHER_OFF = 0, 1
 PME_REAL_F32, PME_REAL_F64 = 0, 1
 

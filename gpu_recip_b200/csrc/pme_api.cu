@@ -54,7 +54,8 @@ struct pme_recip {
   int plane_mode = 0;   // 0 automatic, 1 whole-plane tiles where they fit, 2 separate passes
   int grid_cap = 0;     // CTAs of the persistent launch (0: as many as are resident)
   int x_gather = PME_XGATHER_AUTO;   // PME_XGATHER_*
-  bool accum_zero = true;    // the int64 charge grid is known to be all zero (staged spread skips its clear)
+  bool accum_zero = true;
+  bool no_cluster = false;   // the cluster launch of the plane phase could not be shaped here    // the int64 charge grid is known to be all zero (staged spread skips its clear)
   float* d_force = nullptr;      // pme_eval_host: device forces before the copy to the host
   size_t force_bytes = 0;
 };
@@ -167,6 +168,31 @@ int launch_fused_single(pme_recip* h, const SysDesc& d_in) {
     e = fused_shape(a.total, smem, h->grid_cap, &shape);
   }
   if (e != cudaSuccess) return cuda_fail(e, "fused: launch shape (does the kernel fit on an SM?)");
+  // y, z, the solve and both inverses as kx planes split over 4-CTA clusters, where the plane
+  // count alone would leave most SMs idle (latency build, orthorhombic, line counts divisible);
+  // by default from 32 planes up (64^3: 55.8 against 61.9 us with passes; 32^3 with 17 planes:
+  // 43.5 against 41.5 us with one CTA per plane)
+  const bool want_cluster = h->plane_mode == PME_SCHED_CLUSTER ||
+                            (h->plane_mode == PME_SCHED_AUTO && !d.plane && d.g.hx >= 32);
+  if (want_cluster && !h->no_cluster && shape.variant == kFusedLatency && !d.g.tric && d.g.ny % kClusterPlane == 0 &&
+      d.g.nz % kClusterPlane == 0 && cplane_smem_bytes(d.g.ny, d.g.nz, kClusterPlane) <= kTileSmemBudget) {
+    SysDesc c = d;
+    c.plane = 0;
+    c.cplane = kClusterPlane;
+    int tot[kPhases];
+    fused_tile_counts(c, tot);
+    const size_t csmem = fused_smem_bytes(c);
+    FusedShape cshape;
+    if (fused_shape_cluster(tot, csmem, h->grid_cap, kClusterPlane, &cshape) == cudaSuccess) {
+      d = c;
+      std::memcpy(a.total, tot, sizeof(tot));
+      smem = csmem;
+      shape = cshape;
+    } else {
+      cudaGetLastError();
+      h->no_cluster = true;   // this device cannot hold the cluster launch: never try again
+    }
+  }
   d.gsort = gather_sorts(d, smem);
   a.nbar = fused_barriers(a.total);
   a.single = d;
@@ -198,7 +224,7 @@ void get_config(const pme_recip* h, pme_tune_config* c) {
 
 // Does a shape fit the fused kernel's per-tile shared-memory budget?
 bool config_fits(const SystemState& st, const pme_tune_config& c) {
-  if (c.schedule < PME_SCHED_AUTO || c.schedule > PME_SCHED_PASSES) return false;
+  if (c.schedule < PME_SCHED_AUTO || c.schedule > PME_SCHED_CLUSTER) return false;
   if (c.x_lines < 1 || c.y_lines < 1 || c.z_columns < 1 || c.grid_ctas < 0) return false;
   if (c.x_lines > 64 || c.y_lines > 64 || c.z_columns > 64) return false;
   return tile_smem_bytes(st.nx, c.x_lines) <= kTileSmemBudget && tile_smem_bytes(st.ny, c.y_lines) <= kTileSmemBudget &&
@@ -631,7 +657,7 @@ int pme_set_barrier_spin_limit(pme_recip* h, unsigned int polls) {
 
 int pme_set_fft_schedule(pme_recip* h, int schedule) {
   if (int rc = handle_ok(h)) return rc;
-  if (schedule < PME_SCHED_AUTO || schedule > PME_SCHED_PASSES) return fail(PME_EINVAL, "unknown schedule");
+  if (schedule < PME_SCHED_AUTO || schedule > PME_SCHED_CLUSTER) return fail(PME_EINVAL, "unknown schedule");
   h->plane_mode = schedule;
   return PME_OK;
 }
@@ -996,7 +1022,10 @@ int pme_autotune(pme_recip* h, const void* xyzq, int ncoord, double inv_boxx, do
     bool improved = false;
     for (int knob = 0; knob < 5 && rc == PME_OK; knob++) {
       std::vector<int> vals;
-      if (knob == 0) vals = h->st.plane ? std::vector<int>{PME_SCHED_PLANES, PME_SCHED_PASSES} : std::vector<int>{PME_SCHED_PASSES};
+      if (knob == 0) {
+        vals = h->st.plane ? std::vector<int>{PME_SCHED_PLANES, PME_SCHED_PASSES} : std::vector<int>{PME_SCHED_PASSES};
+        vals.push_back(PME_SCHED_CLUSTER);
+      }
       else if (knob == 1) vals = line_values(best.z_columns);
       else if (knob == 2) vals = line_values(best.y_lines);
       else if (knob == 3) vals = line_values(best.x_lines);

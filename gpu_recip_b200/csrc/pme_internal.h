@@ -87,10 +87,13 @@ enum { kFusedLatency = 0, kFusedThroughput = 1 };
 struct FusedShape {
   int variant;
   int grid;
+  int cluster;   // > 0: launched with thread-block clusters of this many CTAs (latency build)
 };
 // Picks the build and the CTAs (at most the resident maximum, at most the largest phase's tile
 // count, at most grid_cap when > 0) for phases of total[] tiles and smem bytes per CTA.
 cudaError_t fused_shape(const int* total, size_t smem, int grid_cap, FusedShape* out);
 cudaError_t fused_launch(const FusedArgs& a, const FusedShape& shape, size_t smem, cudaStream_t s);
+// The same for a launch with clusters of cs CTAs (the cluster plane tiles).
+cudaError_t fused_shape_cluster(const int* total, size_t smem, int grid_cap, int cs, FusedShape* out);
 
 }  // namespace pme

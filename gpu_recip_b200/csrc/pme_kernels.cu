@@ -13,7 +13,8 @@
 //      4 y inverse (no planes)
 //      5 x inverse (C2R) and the energy/virial finalisation          (cuFFT C2R :2464)
 //      6 gather by bin, writing the bin-sorted atom order            (:1031-1245)
-//    It is compiled twice (latency and throughput builds, see k_fused_lat / k_fused_tput).
+//    It is compiled three times (latency, throughput and cluster builds, see k_fused_lat /
+//    k_fused_tput / k_fused_cl); the cluster build runs phases 2-4 as one phase of cluster plane tiles.
 // Both forms execute the same per-element arithmetic, so forces and energies agree bit for bit.
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -149,8 +150,9 @@ __device__ __forceinline__ int find_system(const int* prefix, int nsys, int t) {
   return lo;
 }
 
-// The fused evaluation's body; compiled twice (see k_fused_lat / k_fused_tput below).
-template <bool LAT>
+// The fused evaluation's body; compiled three times (see k_fused_lat / k_fused_tput / k_fused_cl
+// below).  CL: the build with the cluster plane tiles, launched with 4-CTA clusters.
+template <bool LAT, bool CL = false>
 __device__ __forceinline__ void fused_body(const FusedArgs& a) {
   __shared__ SysDesc d;
   __shared__ int cur;
@@ -189,7 +191,8 @@ __device__ __forceinline__ void fused_body(const FusedArgs& a) {
           break;
         case 1: spread_x_dispatch(d, local, parity, (char*)smem); break;
         case 2:
-          if (d.plane) plane_tile(d, local, smem);
+          if (CL && d.cplane) cplane_tile<kClusterPlane>(d, local, smem);
+          else if (d.plane) plane_tile(d, local, smem);
           else y_tile(d, 0, local, smem);
           break;
         case 3: z_tile(d, 2, local, smem); break;
@@ -232,6 +235,10 @@ __device__ __forceinline__ void fused_body(const FusedArgs& a) {
 // more latency than the spills cost.
 __global__ void __launch_bounds__(kThreads) k_fused_lat(const __grid_constant__ FusedArgs a) { fused_body<true>(a); }
 __global__ void __launch_bounds__(kThreads, 3) k_fused_tput(const __grid_constant__ FusedArgs a) { fused_body<false>(a); }
+// Cluster build: the latency build with the cluster plane tiles, only ever launched with clusters of
+// kClusterPlane CTAs (kept apart so that the other launches run the latency build without the
+// cluster code: compiled into one kernel, it made their evaluations 2-4 us slower).
+__global__ void __launch_bounds__(kThreads) k_fused_cl(const __grid_constant__ FusedArgs a) { fused_body<true, true>(a); }
 
 // ------------------------------- staged cooperative kernel -----------------------------------
 // One reference-interface call (r2c_fft, scalar_sum, c2r_fft) as one cooperative launch over the
@@ -314,9 +321,10 @@ size_t spread_smem(int order) {
 
 size_t fused_smem_bytes(const SysDesc& d) {
   size_t m = 32 * sizeof(long long);
-  size_t c[5] = {staged_fft_smem(d.g.nx, d.tx_rows), staged_fft_smem(d.g.ny, d.tx_y),
+  size_t c[6] = {staged_fft_smem(d.g.nx, d.tx_rows), staged_fft_smem(d.g.ny, d.tx_y),
                  staged_z_smem(d), d.plane ? plane_smem_bytes(d.g.ny, d.g.nz) : 0,
-                 spread_x_smem_bytes(d.g.nx, d.bry * d.brz, d.order)};
+                 spread_x_smem_bytes(d.g.nx, d.bry * d.brz, d.order),
+                 d.cplane ? cplane_smem_bytes(d.g.ny, d.g.nz, d.cplane) : 0};
   for (size_t v : c) m = m > v ? m : v;
   if (d.gx) {
     const size_t v = gx_smem_bytes(d.g.nx, d.bry, d.brz, d.order);
@@ -328,9 +336,9 @@ size_t fused_smem_bytes(const SysDesc& d) {
 void fused_tile_counts(const SysDesc& d, int* counts) {
   counts[0] = tiles_bin(d) + 1;
   counts[1] = tiles_blocks(d);
-  counts[2] = d.plane ? tiles_plane(d) : tiles_ypass(d);
-  counts[3] = d.plane ? 0 : tiles_zpass(d);
-  counts[4] = d.plane ? 0 : tiles_ypass(d);
+  counts[2] = d.cplane ? tiles_plane(d) * d.cplane : (d.plane ? tiles_plane(d) : tiles_ypass(d));
+  counts[3] = (d.plane || d.cplane) ? 0 : tiles_zpass(d);
+  counts[4] = (d.plane || d.cplane) ? 0 : tiles_ypass(d);
   counts[5] = d.gx ? 0 : tiles_xpass(d) + 1;
   counts[6] = tiles_blocks(d) + (d.gx ? 1 : 0);
 }
@@ -487,6 +495,7 @@ cudaError_t fused_shape(const int* total, size_t smem, int grid_cap, FusedShape*
   // many tiles per CTA: more resident CTAs pay; about one: fewer registers per thread cost
   const bool tput = occ_tput > occ_lat && most > 2 * sms * occ_lat;
   out->variant = tput ? kFusedThroughput : kFusedLatency;
+  out->cluster = 0;
   int grid = sms * (tput ? occ_tput : occ_lat);
   grid = grid < most ? grid : most;
   if (grid_cap > 0 && grid > grid_cap) grid = grid_cap;
@@ -494,8 +503,53 @@ cudaError_t fused_shape(const int* total, size_t smem, int grid_cap, FusedShape*
   return grid >= 1 ? cudaSuccess : cudaErrorInvalidConfiguration;
 }
 
+// The cooperative launch of the latency build with thread-block clusters of cs CTAs (the cluster
+// plane tiles): the CTAs that can be co-resident as whole clusters, at most the largest phase's
+// tile count rounded up to whole clusters, at most grid_cap (rounded down to whole clusters).
+static void cluster_config(cudaLaunchConfig_t* cfg, cudaLaunchAttribute* at, int cs, size_t smem, cudaStream_t s) {
+  std::memset(cfg, 0, sizeof(*cfg));
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = (unsigned)cs;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  at[1].id = cudaLaunchAttributeCooperative;
+  at[1].val.cooperative = 1;
+  cfg->gridDim = dim3((unsigned)cs);
+  cfg->blockDim = dim3(kThreads);
+  cfg->dynamicSmemBytes = smem;
+  cfg->stream = s;
+  cfg->attrs = at;
+  cfg->numAttrs = 2;
+}
+
+cudaError_t fused_shape_cluster(const int* total, size_t smem, int grid_cap, int cs, FusedShape* out) {
+  cudaLaunchConfig_t cfg;
+  cudaLaunchAttribute at[2];
+  cluster_config(&cfg, at, cs, smem, nullptr);
+  int ncl = 0;
+  cudaError_t e = cudaOccupancyMaxActiveClusters(&ncl, (const void*)k_fused_cl, &cfg);
+  if (e != cudaSuccess) return e;
+  int most = 1;
+  for (int p = 0; p < kPhases; p++) most = most > total[p] ? most : total[p];
+  int grid = ncl * cs;
+  const int want = (most + cs - 1) / cs * cs;
+  grid = grid < want ? grid : want;
+  if (grid_cap > 0 && grid > grid_cap) grid = grid_cap / cs * cs;
+  out->variant = kFusedLatency;
+  out->grid = grid;
+  out->cluster = cs;
+  return grid >= cs ? cudaSuccess : cudaErrorInvalidConfiguration;
+}
+
 cudaError_t fused_launch(const FusedArgs& a, const FusedShape& shape, size_t smem, cudaStream_t s) {
   FusedArgs args = a;
+  if (shape.cluster > 0) {
+    cudaLaunchConfig_t cfg;
+    cudaLaunchAttribute at[2];
+    cluster_config(&cfg, at, shape.cluster, smem, s);
+    cfg.gridDim = dim3((unsigned)shape.grid);
+    return cudaLaunchKernelEx(&cfg, k_fused_cl, args);
+  }
   void* params[] = {&args};
   return cudaLaunchCooperativeKernel(fused_kernel(shape.variant), dim3(shape.grid), dim3(kThreads), params, smem, s);
 }
@@ -520,6 +574,7 @@ cudaError_t configure_kernels(size_t* max_dyn_smem) {
   if ((e = opt_in_smem(k_spread, optin)) != cudaSuccess) return e;
   if ((e = opt_in_smem(k_fused_lat, optin)) != cudaSuccess) return e;
   if ((e = opt_in_smem(k_fused_tput, optin)) != cudaSuccess) return e;
+  if ((e = opt_in_smem(k_fused_cl, optin)) != cudaSuccess) return e;
   if ((e = opt_in_smem(k_staged, optin)) != cudaSuccess) return e;
   cudaFuncAttributes fa;
   if ((e = cudaFuncGetAttributes(&fa, k_fused_lat)) != cudaSuccess) return e;

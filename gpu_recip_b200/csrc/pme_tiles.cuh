@@ -12,6 +12,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <cooperative_groups.h>
+
 #include "pme_common.cuh"
 #include "pme_fft.cuh"
 
@@ -63,6 +65,8 @@ struct SysDesc {
   double* ev_mirror;         // optional device-mapped host copy of each evaluation's own record
   int tx_rows, tx_y, tx_z;   // lines per tile of the x, y, z passes
   int plane;                 // 1: the fused path runs y, z and the solve as whole-plane tiles
+  int cplane;                // > 0: ... as kx planes split over a thread-block cluster of this
+                             // many CTAs (cplane_tile), in a launch with that cluster size
   int bin_atoms;             // atoms per bin tile of the fused path (0: kThreads)
   int xyzq_host;             // 1: xyzq is pinned host memory, read once in index order
   int gx;                    // 1: each gather tile runs the inverse x pass of the rows it reads
@@ -666,6 +670,99 @@ __device__ __forceinline__ void plane_tile(const SysDesc& d, int kx, float2* sme
   __syncthreads();
   step_mark(d, 14);
 }
+
+// ---------------------------------------------------------------------------------------------
+// Whole kx plane over a thread-block cluster of CS CTAs (orthorhombic boxes): y forward, z forward,
+// solve with energy/virial, z inverse, y inverse in one tile, the two transposes between the y and
+// z lines going through distributed shared memory instead of the global grid and two grid
+// barriers.  Rank r of the cluster owns the z-lines [r nzl, (r+1) nzl) (y transforms, lines of ny
+// elements, A[t (ny+1) + y]) and the y-columns [r nyl, (r+1) nyl) (z transforms and the solve,
+// B[j (nz+1) + z]).  Every line goes through fft_tile and every element through solve_elem as in
+// the pass and plane tiles, so the results are the same bits.  The CS CTAs of a cluster take the
+// same planes in the same order (tile t = CS kx + rank, t = blockIdx.x + k gridDim.x with gridDim.x
+// a multiple of CS), so each cluster barrier is reached by all of them.
+// ---------------------------------------------------------------------------------------------
+__host__ __device__ inline int cplane_lines(int n, int cs) { return (n + cs - 1) / cs; }
+__host__ __device__ inline size_t cplane_smem_bytes(int ny, int nz, int cs) {
+  const size_t A = (size_t)cplane_lines(nz, cs) * (ny + 1), B = (size_t)cplane_lines(ny, cs) * (nz + 1);
+  return sizeof(float2) * ((size_t)ny + nz + 2 * A + 2 * B) + 32 * 7 * sizeof(long long) +
+         4 * sizeof(float) * ((size_t)ny + nz);
+}
+
+constexpr int kClusterPlane = 4;   // CTAs per cluster of the cluster plane tiles
+
+template <int CS>
+__device__ __forceinline__ void cplane_tile(const SysDesc& d, int tile, float2* smem) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cl = cg::this_cluster();
+  const Geom& g = d.g;
+  const int ny = g.ny, nz = g.nz, kx = tile / CS, rank = tile - kx * CS;
+  const int nzl = cplane_lines(nz, CS), nyl = cplane_lines(ny, CS);
+  const int LDA = ny + 1, LDB = nz + 1;
+  const int z0 = rank * nzl, y0 = rank * nyl;
+  const int mz = min(nzl, nz - z0), my = min(nyl, ny - y0);   // lines this rank owns
+  float2* twy = smem;
+  float2* twz = twy + ny;
+  float2* A0 = twz + nz;
+  float2* A1 = A0 + (size_t)nzl * LDA;
+  float2* B0 = A1 + (size_t)nzl * LDA;
+  float2* B1 = B0 + (size_t)nyl * LDB;
+  long long* red = (long long*)(B1 + (size_t)nyl * LDB);
+  float* ksm = (float*)(red + 32 * 7);
+  const int tid = threadIdx.x;
+  float2* __restrict__ base = d.cgrid + cidx(g, kx, 0, 0);
+  const KTab kt = stage_ktab(d, kx, ksm);
+  for (int i = tid; i < ny; i += kThreads) twy[i] = __ldg(&d.tw[d.py.tw_off + i]);
+  for (int i = tid; i < nz; i += kThreads) twz[i] = __ldg(&d.tw[d.pz.tw_off + i]);
+  const FastDiv nyd = d.py.n_div;
+  for (int idx = tid; idx < mz * ny; idx += kThreads) {       // my z-lines, contiguous in y
+    const int t = fdiv(idx, nyd), y = idx - t * ny;
+    A0[t * LDA + y] = __ldcg(&base[(size_t)(z0 + t) * ny + y]);
+  }
+  __syncthreads();
+  float2* ar = fft_tile(A0, A1, d.py, 1, LDA, TileLane(tid, kThreads, nzl), twy, false);
+  // transpose 1: element (z, y) to rank y / nyl, column y - owner nyl, position z
+  const FastDiv nzld = make_fastdiv(nzl);
+  for (int idx = tid; idx < nzl * ny; idx += kThreads) {
+    const int y = fdiv(idx, nzld), t = idx - y * nzl;
+    if (t < mz) {
+      const int owner = y / nyl, j = y - owner * nyl;
+      float2* dst = cl.map_shared_rank(B0 + (size_t)j * LDB + (z0 + t), owner);
+      *dst = ar[t * LDA + y];
+    }
+  }
+  cl.sync();
+  float2* br = fft_tile(B0, B1, d.pz, 1, LDB, TileLane(tid, kThreads, nyl), twz, false);
+  {
+    long long acc[7] = {0, 0, 0, 0, 0, 0, 0};
+    const FastDiv nzd = d.pz.n_div;
+    for (int idx = tid; idx < my * nz; idx += kThreads) {
+      const int j = fdiv(idx, nzd), z = idx - j * nz;
+      solve_elem(br[j * LDB + z], kx, y0 + j, z, d, kt, acc);
+    }
+    if (d.calc_ev) flush_ev(d, acc, red);
+  }
+  __syncthreads();
+  float2* bi = fft_tile(br, br == B0 ? B1 : B0, d.pz, 1, LDB, TileLane(tid, kThreads, nyl), twz, true);
+  // transpose 2: element (y, z) back to rank z / nzl, line z - owner nzl, position y
+  const FastDiv nyld = make_fastdiv(nyl);
+  for (int idx = tid; idx < nyl * nz; idx += kThreads) {
+    const int z = fdiv(idx, nyld), j = idx - z * nyl;
+    if (j < my) {
+      const int owner = z / nzl, t = z - owner * nzl;
+      float2* dst = cl.map_shared_rank(A0 + (size_t)t * LDA + (y0 + j), owner);
+      *dst = bi[j * LDB + z];
+    }
+  }
+  cl.sync();
+  float2* yr = fft_tile(A0, A1, d.py, 1, LDA, TileLane(tid, kThreads, nzl), twy, true);
+  for (int idx = tid; idx < mz * ny; idx += kThreads) {
+    const int t = fdiv(idx, nyd), y = idx - t * ny;
+    __stcg(&base[(size_t)(z0 + t) * ny + y], yr[t * LDA + y]);
+  }
+  __syncthreads();
+}
+
 
 // ---------------------------------------------------------------------------------------------
 // Fused path, phase 0: bin kThreads atoms by the row block of their stencil origin; sum q^2.

@@ -310,7 +310,7 @@ class CudaPMERecip:
             C.check(self._lib.pme_set_trace(self._h, _ptr(buf), int(max_ctas or buf.numel() // 14)), "set_trace")
 
     def set_fft_schedule(self, schedule: int):
-        """PME_SCHED_AUTO / PME_SCHED_PLANES / PME_SCHED_PASSES (identical results)."""
+        """PME_SCHED_AUTO / PME_SCHED_PLANES / PME_SCHED_PASSES / PME_SCHED_CLUSTER (identical results)."""
         C.check(self._lib.pme_set_fft_schedule(self._h, int(schedule)), "set_fft_schedule")
 
     def set_x_gather_fusion(self, mode: int):

@@ -198,9 +198,13 @@ PME_API int pme_set_barrier_spin_limit(pme_recip* h, unsigned int polls);   /* d
 PME_API int pme_reserve_atoms(pme_recip* h, int natom);
 /* Schedule of the fused evaluation's y/z transforms: PME_SCHED_PLANES runs y, z and the solve
  * as whole-plane tiles (one CTA per kx plane, where a plane fits in shared memory),
- * PME_SCHED_PASSES as separate y and z passes (more, smaller tiles), PME_SCHED_AUTO (default)
- * picks planes only when there are at least as many planes as SMs.  Results are identical. */
-enum { PME_SCHED_AUTO = 0, PME_SCHED_PLANES = 1, PME_SCHED_PASSES = 2 };
+ * PME_SCHED_PASSES as separate y and z passes (more, smaller tiles), PME_SCHED_CLUSTER as kx
+ * planes split over a cluster of 4 CTAs (y lines and z lines exchanged through distributed shared
+ * memory; single systems in the latency build, orthorhombic boxes, ny and nz multiples of 4, else
+ * passes), PME_SCHED_AUTO (default) picks planes when there are at least as many planes as SMs,
+ * else the cluster form where it applies and there are at least 32 planes, else passes.  Results
+ * are identical. */
+enum { PME_SCHED_AUTO = 0, PME_SCHED_PLANES = 1, PME_SCHED_PASSES = 2, PME_SCHED_CLUSTER = 3 };
 
 /* ---- autotuner ----
  * No counterpart in the reference (its launch shapes are fixed).  The fused evaluation's launch
