@@ -37,6 +37,7 @@ __device__ __forceinline__ int fdiv(int x, const FastDiv& f) {
 
 struct FftPlan1D {
   int n;                    // transform length
+  int code;                 // > 0: a length with a compile-time stage sequence (fft_tile)
   int nstages;
   int radix[kMaxStages];
   FastDiv ns_div[kMaxStages];   // division by the stage's sub-transform length Ns
@@ -175,6 +176,57 @@ __device__ __forceinline__ void fft_stage(const float2* __restrict__ in, float2*
   }
 }
 
+// One Stockham stage with the radix, the sub-transform length NS and the line length L known at
+// compile time: the same butterflies and the same roundings as fft_stage, with constant index
+// arithmetic.
+template <int R, int NS, int L>
+__device__ __forceinline__ void fft_stage_ct(const float2* __restrict__ in, float2* __restrict__ out, int es, int ls,
+                                             const TileLane& ln, const float2* tw, bool inv) {
+  constexpr int nb = L / R;
+  constexpr int tstride = L / (NS * R);
+  const int lo = ln.t * ls;
+  if (!ln.active()) return;
+  for (int j = ln.y; j < nb; j += ln.ny) {
+    const int blk = j / NS;
+    const int k = j - blk * NS;
+    float2 v[R];
+#pragma unroll
+    for (int r = 0; r < R; r++) v[r] = in[(j + r * nb) * es + lo];
+#pragma unroll
+    for (int r = 1; r < R; r++) {
+      float2 w = tw[r * k * tstride];
+      if (inv) w.y = -w.y;
+      v[r] = cmul(v[r], w);
+    }
+    dft_small<R>(v, inv);
+    const int base = blk * NS * R + k;
+#pragma unroll
+    for (int u = 0; u < R; u++) out[(base + u * NS) * es + lo] = v[u];
+  }
+}
+
+// The stages R, Rest... of a length-L transform from sub-transform length NS on, unrolled at
+// compile time; returns the buffer holding the result.
+template <int L, int NS, int R, int... Rest>
+__device__ __forceinline__ float2* fft_seq_ct(float2* src, float2* dst, int es, int ls, const TileLane& ln,
+                                              const float2* tw, bool inv) {
+  fft_stage_ct<R, NS, L>(src, dst, es, ls, ln, tw, inv);
+  __syncthreads();
+  if constexpr (sizeof...(Rest) == 0) {
+    return dst;
+  } else {
+    return fft_seq_ct<L, NS * R, Rest...>(dst, src, es, ls, ln, tw, inv);
+  }
+}
+
+// Lengths with a compile-time stage sequence (FftPlan1D::code): a generic stage loop with a
+// runtime radix costs about three times the cycles of the same stages unrolled (measured on a
+// 16 x 64 tile: 2,390 against 730 cycles per transform).
+enum { kFftGeneric = 0, kFft64 = 1, kFft32 = 2, kFft216 = 3 };
+__host__ __device__ inline int fft_code(int n) {
+  return n == 64 ? kFft64 : (n == 32 ? kFft32 : (n == 216 ? kFft216 : kFftGeneric));
+}
+
 // Full transform of every line of the tile held in buf0 (element stride es, line stride ls);
 // returns the buffer that holds the result (buf0 or buf1).  Every thread of the CTA must call
 // it; it synchronises between stages and before returning.  Not inlined: the fused evaluation
@@ -183,6 +235,12 @@ __device__ __forceinline__ void fft_stage(const float2* __restrict__ in, float2*
 static __device__ __noinline__ float2* fft_tile(float2* buf0, float2* buf1, const FftPlan1D& plan,
                                          int es, int ls, const TileLane ln, const float2* tw,
                                          bool inv) {
+  switch (plan.code) {   // factorize() orders the radices 8, 4, 2, 3, 5
+    case kFft64: return fft_seq_ct<64, 1, 8, 8>(buf0, buf1, es, ls, ln, tw, inv);
+    case kFft32: return fft_seq_ct<32, 1, 8, 4>(buf0, buf1, es, ls, ln, tw, inv);
+    case kFft216: return fft_seq_ct<216, 1, 8, 3, 3, 3>(buf0, buf1, es, ls, ln, tw, inv);
+    default: break;
+  }
   float2* src = buf0;
   float2* dst = buf1;
   int Ns = 1;

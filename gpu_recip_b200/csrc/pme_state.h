@@ -40,6 +40,7 @@ struct DeviceGuard {
 
 inline bool factorize(int n, FftPlan1D& p) {
   p.n = n;
+  p.code = fft_code(n);
   p.nstages = 0;
   p.n_div = make_fastdiv(n);
   int m = n;

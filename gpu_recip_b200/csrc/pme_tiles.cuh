@@ -89,7 +89,8 @@ struct SysDesc {
 
 // Profiling stamp of one step of a tile (CTA 0, thread 0 only; no-op when steps is null).
 // Slots: 0-6 the spread + x tile (start, candidates counted, first round listed, spreading done,
-// rows converted, x FFT done, stored), 8-14 the plane tile, 16-21 the bin tile, 24-26 the gather
+// rows converted, x FFT done, stored), 8-14 the plane tile (or the cluster plane tile: start,
+// loaded, y FFT, transposed, solved, transposed back, done), 16-21 the bin tile, 24-26 the gather
 // tile; a CTA that runs several tiles of a phase leaves the stamps of its last one.
 __device__ __forceinline__ void step_mark(const SysDesc& d, int slot) {
   if (d.steps != nullptr && blockIdx.x == 0 && threadIdx.x == 0) {
@@ -711,6 +712,7 @@ __device__ __forceinline__ void cplane_tile(const SysDesc& d, int tile, float2* 
   float* ksm = (float*)(red + 32 * 7);
   const int tid = threadIdx.x;
   float2* __restrict__ base = d.cgrid + cidx(g, kx, 0, 0);
+  step_mark(d, 8);
   const KTab kt = stage_ktab(d, kx, ksm);
   for (int i = tid; i < ny; i += kThreads) twy[i] = __ldg(&d.tw[d.py.tw_off + i]);
   for (int i = tid; i < nz; i += kThreads) twz[i] = __ldg(&d.tw[d.pz.tw_off + i]);
@@ -720,7 +722,9 @@ __device__ __forceinline__ void cplane_tile(const SysDesc& d, int tile, float2* 
     A0[t * LDA + y] = __ldcg(&base[(size_t)(z0 + t) * ny + y]);
   }
   __syncthreads();
+  step_mark(d, 9);
   float2* ar = fft_tile(A0, A1, d.py, 1, LDA, TileLane(tid, kThreads, nzl), twy, false);
+  step_mark(d, 10);
   // transpose 1: element (z, y) to rank y / nyl, column y - owner nyl, position z
   const FastDiv nzld = make_fastdiv(nzl);
   for (int idx = tid; idx < nzl * ny; idx += kThreads) {
@@ -732,6 +736,7 @@ __device__ __forceinline__ void cplane_tile(const SysDesc& d, int tile, float2* 
     }
   }
   cl.sync();
+  step_mark(d, 11);
   float2* br = fft_tile(B0, B1, d.pz, 1, LDB, TileLane(tid, kThreads, nyl), twz, false);
   {
     long long acc[7] = {0, 0, 0, 0, 0, 0, 0};
@@ -743,6 +748,7 @@ __device__ __forceinline__ void cplane_tile(const SysDesc& d, int tile, float2* 
     if (d.calc_ev) flush_ev(d, acc, red);
   }
   __syncthreads();
+  step_mark(d, 12);
   float2* bi = fft_tile(br, br == B0 ? B1 : B0, d.pz, 1, LDB, TileLane(tid, kThreads, nyl), twz, true);
   // transpose 2: element (y, z) back to rank z / nzl, line z - owner nzl, position y
   const FastDiv nyld = make_fastdiv(nyl);
@@ -755,12 +761,14 @@ __device__ __forceinline__ void cplane_tile(const SysDesc& d, int tile, float2* 
     }
   }
   cl.sync();
+  step_mark(d, 13);
   float2* yr = fft_tile(A0, A1, d.py, 1, LDA, TileLane(tid, kThreads, nzl), twy, true);
   for (int idx = tid; idx < mz * ny; idx += kThreads) {
     const int t = fdiv(idx, nyd), y = idx - t * ny;
     __stcg(&base[(size_t)(z0 + t) * ny + y], yr[t * LDA + y]);
   }
   __syncthreads();
+  step_mark(d, 14);
 }
 
 
