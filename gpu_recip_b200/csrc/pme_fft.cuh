@@ -222,9 +222,49 @@ __device__ __forceinline__ float2* fft_seq_ct(float2* src, float2* dst, int es, 
 // Lengths with a compile-time stage sequence (FftPlan1D::code): a generic stage loop with a
 // runtime radix costs about three times the cycles of the same stages unrolled (measured on a
 // 16 x 64 tile: 2,390 against 730 cycles per transform).
-enum { kFftGeneric = 0, kFft64 = 1, kFft32 = 2, kFft216 = 3 };
+// The lengths are those of the benchmarked grids: 32, 64, 216 and the 24-60 of the batch.
+enum {
+  kFftGeneric = 0, kFft64, kFft32, kFft216, kFft24, kFft25, kFft27, kFft30, kFft36, kFft40, kFft45, kFft48,
+  kFft50, kFft54, kFft60
+};
 __host__ __device__ inline int fft_code(int n) {
-  return n == 64 ? kFft64 : (n == 32 ? kFft32 : (n == 216 ? kFft216 : kFftGeneric));
+  switch (n) {
+    case 64: return kFft64;
+    case 32: return kFft32;
+    case 216: return kFft216;
+    case 24: return kFft24;
+    case 25: return kFft25;
+    case 27: return kFft27;
+    case 30: return kFft30;
+    case 36: return kFft36;
+    case 40: return kFft40;
+    case 45: return kFft45;
+    case 48: return kFft48;
+    case 50: return kFft50;
+    case 54: return kFft54;
+    case 60: return kFft60;
+    default: return kFftGeneric;
+  }
+}
+
+// The batch lengths (24-60), in a function of their own that fft_tile calls: fft_tile's dispatch
+// for 64, 32 and 216 stays a short compare chain (one switch over all fourteen lengths cost the
+// 32^3 evaluation 2 us).
+static __device__ __noinline__ float2* fft_tile_batch(float2* buf0, float2* buf1, int code, int es, int ls,
+                                                      const TileLane ln, const float2* tw, bool inv) {
+  switch (code) {
+    case kFft24: return fft_seq_ct<24, 1, 8, 3>(buf0, buf1, es, ls, ln, tw, inv);
+    case kFft25: return fft_seq_ct<25, 1, 5, 5>(buf0, buf1, es, ls, ln, tw, inv);
+    case kFft27: return fft_seq_ct<27, 1, 3, 3, 3>(buf0, buf1, es, ls, ln, tw, inv);
+    case kFft30: return fft_seq_ct<30, 1, 2, 3, 5>(buf0, buf1, es, ls, ln, tw, inv);
+    case kFft36: return fft_seq_ct<36, 1, 4, 3, 3>(buf0, buf1, es, ls, ln, tw, inv);
+    case kFft40: return fft_seq_ct<40, 1, 8, 5>(buf0, buf1, es, ls, ln, tw, inv);
+    case kFft45: return fft_seq_ct<45, 1, 3, 3, 5>(buf0, buf1, es, ls, ln, tw, inv);
+    case kFft48: return fft_seq_ct<48, 1, 8, 2, 3>(buf0, buf1, es, ls, ln, tw, inv);
+    case kFft50: return fft_seq_ct<50, 1, 2, 5, 5>(buf0, buf1, es, ls, ln, tw, inv);
+    case kFft54: return fft_seq_ct<54, 1, 2, 3, 3, 3>(buf0, buf1, es, ls, ln, tw, inv);
+    default: return fft_seq_ct<60, 1, 4, 3, 5>(buf0, buf1, es, ls, ln, tw, inv);
+  }
 }
 
 // Full transform of every line of the tile held in buf0 (element stride es, line stride ls);
@@ -241,6 +281,7 @@ static __device__ __noinline__ float2* fft_tile(float2* buf0, float2* buf1, cons
     case kFft216: return fft_seq_ct<216, 1, 8, 3, 3, 3>(buf0, buf1, es, ls, ln, tw, inv);
     default: break;
   }
+  if (plan.code >= kFft24) return fft_tile_batch(buf0, buf1, plan.code, es, ls, ln, tw, inv);
   float2* src = buf0;
   float2* dst = buf1;
   int Ns = 1;
