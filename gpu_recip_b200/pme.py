@@ -47,6 +47,23 @@ def force_stride(n: int, itemsize: int = 4) -> int:
     return ((((n - 1 + 32) * itemsize) - 1) // 256 + 1) * 256 // itemsize
 
 
+TRACE_STEP_STAMPS = 32   # entries after the per-CTA phase stamps of a single-system trace
+
+
+def _trace_ctas(buf, max_ctas: int, extra: int) -> int:
+    """CTAs a trace buffer of buf.numel() int64 entries holds (14 each, then `extra`); a
+    max_ctas that does not fit raises instead of letting the kernel write past the buffer."""
+    import torch
+    if buf.dtype != torch.int64 or not buf.is_cuda:
+        raise ValueError("trace buffer must be an int64 CUDA tensor")
+    fit = (buf.numel() - extra) // 14
+    n = int(max_ctas) if max_ctas else fit
+    if n < 1 or n > fit:
+        raise ValueError(f"trace buffer of {buf.numel()} entries holds {max(fit, 0)} CTAs (14 entries each"
+                         f" + {extra}); asked for {n}")
+    return n
+
+
 def _stream_handle(stream) -> int:
     if stream is None:
         return 0
@@ -303,11 +320,12 @@ class CudaPMERecip:
 
     def set_trace(self, buf, max_ctas: int = 0):
         """Record per-CTA, per-phase %globaltimer stamps of fused evaluations into ``buf`` (int64
-        device tensor of max_ctas*14 entries); None turns it off."""
+        device tensor of max_ctas*14 entries plus 32 step stamps of CTA 0); None turns it off."""
         if buf is None:
             C.check(self._lib.pme_set_trace(self._h, None, 0), "set_trace")
         else:
-            C.check(self._lib.pme_set_trace(self._h, _ptr(buf), int(max_ctas or buf.numel() // 14)), "set_trace")
+            n = _trace_ctas(buf, max_ctas, TRACE_STEP_STAMPS)
+            C.check(self._lib.pme_set_trace(self._h, _ptr(buf), n), "set_trace")
 
     def set_fft_schedule(self, schedule: int):
         """PME_SCHED_AUTO / PME_SCHED_PLANES / PME_SCHED_PASSES / PME_SCHED_CLUSTER (identical results)."""
@@ -447,10 +465,12 @@ class PmeBatch:
         return out
 
     def set_trace(self, buf, max_ctas: int = 0):
+        """Per-CTA, per-phase stamps of the batch launch into ``buf`` (int64 device tensor of at
+        least max_ctas*14 entries); None turns it off."""
         if buf is None:
             C.check(self._lib.pme_batch_set_trace(self._h, None, 0), "set_trace")
         else:
-            C.check(self._lib.pme_batch_set_trace(self._h, _ptr(buf), int(max_ctas or buf.numel() // 14)), "set_trace")
+            C.check(self._lib.pme_batch_set_trace(self._h, _ptr(buf), _trace_ctas(buf, max_ctas, 0)), "set_trace")
 
     def autotune(self, reps: int = 5) -> dict:
         """Measure the batch's y/z schedule and launch size and keep the fastest."""
