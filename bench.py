@@ -68,7 +68,30 @@ def parse():
                     help="further single-system workloads timed beside the main one")
     ap.add_argument("--also-steps", type=int, default=200)
     ap.add_argument("--no-fft-comparator", dest="fft_comparator", action="store_false")
+    ap.add_argument("--fft-schedule", default="auto", choices=list(SCHEDULES),
+                    help="auto: the autotuner picks the launch shape; otherwise that y/z schedule with default "
+                         "tiles and no autotuning (profilers that cannot launch thread-block clusters)")
     return ap.parse_args()
+
+
+SCHEDULES = {"auto": 0, "planes": 1, "passes": 2, "cluster": 3}
+
+
+def new_handle(args, nfft, order, stream=None):
+    """A CudaPMERecip with the y/z schedule pinned from its first evaluation when --fft-schedule
+    asks for one."""
+    from gpu_recip_b200 import CudaPMERecip
+    pme = CudaPMERecip(*nfft, order, stream=stream)
+    if args.fft_schedule != "auto":
+        pme.set_fft_schedule(SCHEDULES[args.fft_schedule])
+    return pme
+
+
+def tune_single(pme, args, inv_box, x, n, kappa, reps):
+    """The autotuner's launch shape, or (--fft-schedule) the pinned y/z schedule with default tiles."""
+    if args.fft_schedule == "auto":
+        return pme.autotune(inv_box, x, n, kappa, reps=reps)
+    return dict(pme.get_tune_config(), schedule=SCHEDULES[args.fft_schedule], pinned=True)
 
 
 def make_workload(name: str, rank: int = 0):
@@ -304,7 +327,7 @@ def run_b200(args):
     n = s.natom
     stride = force_stride(n)
     stream = torch.cuda.Stream(device=dev)
-    pme = CudaPMERecip(*s.nfft, s.order, stream=stream)
+    pme = new_handle(args, s.nfft, s.order, stream)
     inv_box = [1.0 / b for b in s.box]
     recip = [inv_box[0], 0, 0, 0, inv_box[1], 0, 0, 0, inv_box[2]]
     x_dev = torch.from_numpy(s.xyzq).to(dev)
@@ -327,7 +350,7 @@ def run_b200(args):
             one_eval()
     stream.synchronize()
     # launch shape of the fused kernel from the autotuner (results are the same for every shape)
-    tune = pme.autotune(inv_box, x_dev, n, s.kappa, reps=10)
+    tune = tune_single(pme, args, inv_box, x_dev, n, s.kappa, 10)
     with torch.cuda.stream(stream):
         for _ in range(3):
             flush.fill_(0.0)
@@ -479,11 +502,11 @@ def run_single(name, args, dev, stream, flush, rank, world):
     s = make_workload(name, rank)
     n = s.natom
     stride = force_stride(n)
-    pme = CudaPMERecip(*s.nfft, s.order, stream=stream)
+    pme = new_handle(args, s.nfft, s.order, stream)
     inv_box = [1.0 / b for b in s.box]
     x = torch.from_numpy(s.xyzq).to(dev)
     f = torch.zeros(3 * stride, dtype=torch.float32, device=dev)
-    tune = pme.autotune(inv_box, x, n, s.kappa, reps=10)
+    tune = tune_single(pme, args, inv_box, x, n, s.kappa, 10)
     K = args.also_steps
     W = max(3, args.warmup)
     e0 = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
@@ -567,7 +590,7 @@ def run_batched(args, dev, stream, flush, rank, world):
             "evals_per_s": R.aggregate_rate([len(systems) * K] * world, total / 1000.0), "ms_per_batch": ms,
             "p50_ms": float(np.percentile(per, 50)), "p99_ms": float(np.percentile(per, 99)),
             "launches_per_batch": 1, "cuda_graph": True, "grid_ctas": info["grid_ctas"],
-            "autotune": {"schedule": ["auto", "planes", "passes"][tune["schedule"]], "grid_ctas": tune["grid_ctas"],
+            "autotune": {"schedule": ["auto", "planes", "passes", "cluster"][tune["schedule"]], "grid_ctas": tune["grid_ctas"],
                          "line_scale": tune["x_lines"], "candidates": tune["candidates"]},
             "device_bytes": info["device_bytes"], "alg_bytes_per_batch": alg,
             "roofline_frac": alg / (ms * 1e-3) / 1e9 / peak,
@@ -630,12 +653,12 @@ def run_large(args, dev, stream, flush, rank, world):
     s = S.config_large(seed=R.replica_seed(3, rank))
     n = s.natom
     st = force_stride(n)
-    pme = CudaPMERecip(*s.nfft, s.order, stream=stream)
+    pme = new_handle(args, s.nfft, s.order, stream)
     inv_box = [1.0 / b for b in s.box]
     recip = [inv_box[0], 0, 0, 0, inv_box[1], 0, 0, 0, inv_box[2]]
     x = torch.from_numpy(s.xyzq).to(dev)
     f = torch.zeros(3 * st, dtype=torch.float32, device=dev)
-    tune = pme.autotune(inv_box, x, n, s.kappa, reps=3)
+    tune = tune_single(pme, args, inv_box, x, n, s.kappa, 3)
     K = args.large_steps
     ev0 = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
     ev1 = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
@@ -780,7 +803,7 @@ def run_triclinic(args, dev, stream, flush, rank, world):
     s = S.config_triclinic(4, seed=R.replica_seed(6, rank))
     n = s.natom
     st = force_stride(n)
-    pme = CudaPMERecip(*s.nfft, s.order, stream=stream)
+    pme = new_handle(args, s.nfft, s.order, stream)
     x = torch.from_numpy(s.xyzq).to(dev)
     f = torch.zeros(3 * st, dtype=torch.float32, device=dev)
     r9 = s.recip9
@@ -832,7 +855,7 @@ def run_direct(args, dev, stream, flush, rank, world):
     x = torch.from_numpy(np.ascontiguousarray(d["xyzq"], dtype=np.float32)).to(dev)
     stride = force_stride(n, 8)
     fi = torch.zeros(3 * stride, dtype=torch.int64, device=dev)
-    pme = CudaPMERecip(64, 64, 64, 4, stream=stream)
+    pme = new_handle(args, (64, 64, 64), 4, stream)
     inv = [1.0 / float(b) for b in d["box"]]
     K = args.direct_steps
     W = max(3, args.warmup)
@@ -953,7 +976,7 @@ def run_serving(args, dev, rank, world):
     for sy in pool:
         key = (tuple(sy.nfft), sy.order)
         if key not in handles:
-            handles[key] = CudaPMERecip(*sy.nfft, sy.order, stream=stream)
+            handles[key] = new_handle(args, sy.nfft, sy.order, stream)
 
     def plain(rate_arrivals):
         lat = []
