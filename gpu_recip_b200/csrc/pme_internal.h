@@ -47,7 +47,7 @@ int fused_barriers(const int* total);
 // kStgXFwdZero reads the int64 charge grid and leaves it zero behind it (ready for the next
 // atomic spread).
 enum StagedKind {
-  kStgXFwdZero = 0, kStgYFwd, kStgZFwd, kStgKtab, kStgZSolve, kStgFinalizeSolve, kStgZInv, kStgYInv, kStgXInv
+  kStgXFwdZero = 0, kStgYFwd, kStgZFwd, kStgZSolve, kStgZInv, kStgYInv, kStgXInv
 };
 constexpr int kStagedMaxPhases = 4;
 
@@ -59,6 +59,7 @@ struct StagedArgs {
   unsigned long long* bar;   // the handle's barrier words (shared with its fused evaluations)
   int* status;
   unsigned int spin_limit;
+  unsigned int* ticket;      // non-null: the last CTA to finish finalises the solve's record
 };
 
 // The handle's barrier words and failure-detection settings for a staged launch.

@@ -259,11 +259,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_staged(const __grid_constant__ 
         case kStgXFwdZero: x_fwd_tile(d, t, smem, true); break;
         case kStgYFwd: y_tile(d, 0, t, smem); break;
         case kStgZFwd: z_tile(d, 0, t, smem); break;
-        case kStgKtab: ktab_tile(d); break;
         case kStgZSolve: z_tile(d, 3, t, smem); break;
-        case kStgFinalizeSolve:
-          if (threadIdx.x == 0) finalize_system(d, true, false);
-          break;
         case kStgZInv: z_tile(d, 1, t, smem); break;
         case kStgYInv: y_tile(d, 1, t, smem); break;
         default: x_inv_tile(d, t, smem); break;
@@ -271,6 +267,21 @@ __global__ void __launch_bounds__(kThreads, 2) k_staged(const __grid_constant__ 
       __syncthreads();
     }
     if (ph < nbar && !grid_barrier(a.bar, base, ph, nbar, a.status, a.spin_limit, false)) return;
+  }
+  if (a.ticket != nullptr) {
+    // the energy/virial sums of every CTA are in the accumulators once all have taken a ticket
+    __shared__ bool last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      last = atomicAdd(a.ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+      __threadfence();
+      finalize_system(d, true, false);
+      *a.ticket = 0u;
+    }
   }
 }
 
@@ -357,8 +368,10 @@ cudaError_t staged_spread(const SysDesc& d, cudaStream_t s) {
 }
 
 cudaError_t staged_self(const SysDesc& d, unsigned int* done, cudaStream_t s) {
-  int blocks = (d.natom + 4 * kThreads - 1) / (4 * kThreads);
-  blocks = blocks < 1 ? 1 : (blocks > 592 ? 592 : blocks);
+  // one charge per thread up to 1184 CTAs: the sum is latency-bound (24,000 charges: 24 CTAs of
+  // four loads per thread took 6.2 us with caches cold)
+  int blocks = (d.natom + kThreads - 1) / kThreads;
+  blocks = blocks < 1 ? 1 : (blocks > 1184 ? 1184 : blocks);
   k_self_energy<<<blocks, kThreads, 0, s>>>(d, done);
   return cudaGetLastError();
 }
@@ -378,11 +391,12 @@ static int staged_phase_tiles(const SysDesc& d, int kind) {
     case kStgXFwdZero: case kStgXInv: return tiles_xpass(d);
     case kStgYFwd: case kStgYInv: return tiles_ypass(d);
     case kStgZFwd: case kStgZSolve: case kStgZInv: return tiles_zpass(d);
-    default: return 1;   // kStgKtab, kStgFinalizeSolve
+    default: return 1;
   }
 }
 
-cudaError_t staged_launch(const SysDesc& d, const int* kinds, int nphase, const StagedCtx& c, cudaStream_t s) {
+cudaError_t staged_launch(const SysDesc& d, const int* kinds, int nphase, const StagedCtx& c, cudaStream_t s,
+                          unsigned int* ticket = nullptr) {
   static std::mutex mu;
   static std::map<std::pair<int, size_t>, int> occ_cache;
   StagedArgs a;
@@ -392,6 +406,7 @@ cudaError_t staged_launch(const SysDesc& d, const int* kinds, int nphase, const 
   a.bar = c.bar;
   a.status = c.status;
   a.spin_limit = c.spin_limit;
+  a.ticket = ticket;
   size_t smem = 32 * sizeof(long long);
   int most = 1;
   for (int p = 0; p < nphase; p++) {
@@ -426,9 +441,11 @@ cudaError_t staged_r2c(const SysDesc& d, const StagedCtx& c, cudaStream_t s) {
   return staged_launch(d, kinds, 3, c, s);
 }
 
+// One phase: every z tile computes the influence tables it needs, and the last CTA to finish
+// writes the record (no grid barrier).  The ticket counter is the handle's barrier word 5.
 cudaError_t staged_solve(const SysDesc& d, const StagedCtx& c, cudaStream_t s) {
-  const int kinds[3] = {kStgKtab, kStgZSolve, kStgFinalizeSolve};
-  return staged_launch(d, kinds, 3, c, s);
+  const int kinds[1] = {kStgZSolve};
+  return staged_launch(d, kinds, 1, c, s, (unsigned int*)(c.bar + 5));
 }
 
 cudaError_t staged_c2r(const SysDesc& d, const StagedCtx& c, cudaStream_t s) {

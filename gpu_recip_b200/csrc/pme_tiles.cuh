@@ -304,27 +304,41 @@ __device__ __forceinline__ void x_inv_tile(const SysDesc& d, int tile, float2* s
 // Table layout (ntot = nx+ny+nz entries each): [0] k_x contribution (mhat_d when orthorhombic),
 // [1] A_d, and for triclinic boxes [2] k_y and [3] k_z contributions.
 // ---------------------------------------------------------------------------------------------
+// Table entry i (x entries, then y, then z): v[0] k contribution (mhat), v[1] A; triclinic boxes
+// also v[2], v[3] (k_y and k_z contributions).
+__device__ __forceinline__ void ktab_entry(const SysDesc& d, int i, double* v) {
+  const Geom& g = d.g;
+  int n, k, ax;
+  double r;
+  if (i < g.nx) { n = g.nx; k = i; r = d.rxd; ax = 0; }
+  else if (i < g.nx + g.ny) { n = g.ny; k = i - g.nx; r = d.ryd; ax = 1; }
+  else { n = g.nz; k = i - g.nx - g.ny; r = d.rzd; ax = 2; }
+  const int nf = (n >> 1) + (n & 1);
+  const int m = k < nf ? k : k - n;
+  if (!g.tric) {
+    const double mh = r * (double)m;
+    v[0] = mh;
+    v[1] = d.bmod[i] * exp(-d.fac * mh * mh);
+  } else {
+    const double md = (double)m;
+    v[0] = d.rm[ax] * md;
+    v[1] = d.bmod[i] * exp(-d.fac * d.gdiag[ax] * md * md);
+    v[2] = d.rm[3 + ax] * md;
+    v[3] = d.rm[6 + ax] * md;
+  }
+}
+
 __device__ __forceinline__ void ktab_tile(const SysDesc& d) {
   const Geom& g = d.g;
   const int ntot = g.nx + g.ny + g.nz;
   for (int i = threadIdx.x; i < ntot; i += kThreads) {
-    int n, k, ax;
-    double r;
-    if (i < g.nx) { n = g.nx; k = i; r = d.rxd; ax = 0; }
-    else if (i < g.nx + g.ny) { n = g.ny; k = i - g.nx; r = d.ryd; ax = 1; }
-    else { n = g.nz; k = i - g.nx - g.ny; r = d.rzd; ax = 2; }
-    const int nf = (n >> 1) + (n & 1);
-    const int m = k < nf ? k : k - n;
-    if (!g.tric) {
-      const double mh = r * (double)m;
-      d.ktab[i] = mh;
-      d.ktab[ntot + i] = d.bmod[i] * exp(-d.fac * mh * mh);
-    } else {
-      const double md = (double)m;
-      d.ktab[i] = d.rm[ax] * md;
-      d.ktab[ntot + i] = d.bmod[i] * exp(-d.fac * d.gdiag[ax] * md * md);
-      d.ktab[2 * ntot + i] = d.rm[3 + ax] * md;
-      d.ktab[3 * ntot + i] = d.rm[6 + ax] * md;
+    double v[4];
+    ktab_entry(d, i, v);
+    d.ktab[i] = v[0];
+    d.ktab[ntot + i] = v[1];
+    if (g.tric) {
+      d.ktab[2 * ntot + i] = v[2];
+      d.ktab[3 * ntot + i] = v[3];
     }
   }
 }
@@ -363,6 +377,35 @@ __device__ __forceinline__ KTab stage_ktab(const SysDesc& d, int kx, float* sm) 
   t.A1 = (float)__ldcg(&d.ktab[ntot + kx]);
   t.m1b = g.tric ? (float)__ldcg(&d.ktab[2 * ntot + kx]) : 0.0f;
   t.m1c = g.tric ? (float)__ldcg(&d.ktab[3 * ntot + kx]) : 0.0f;
+  t.my = sm;
+  t.mz = sm + g.ny;
+  t.Ay = sm + nyz;
+  t.Az = sm + nyz + g.ny;
+  return t;
+}
+
+// stage_ktab with the entries computed in place (ktab_entry, the same FP64 arithmetic as
+// ktab_tile, so the same values), for a solve launch with no table phase before it.
+__device__ __forceinline__ KTab stage_ktab_local(const SysDesc& d, int kx, float* sm) {
+  const Geom& g = d.g;
+  const int nyz = g.ny + g.nz;
+  for (int j = threadIdx.x; j < nyz; j += kThreads) {
+    double v[4];
+    ktab_entry(d, g.nx + j, v);
+    sm[j] = (float)v[0];
+    sm[nyz + j] = (float)v[1];
+    if (g.tric) {
+      sm[2 * nyz + j] = (float)v[2];
+      sm[3 * nyz + j] = (float)v[3];
+    }
+  }
+  double vx[4];
+  ktab_entry(d, kx, vx);
+  KTab t;
+  t.m1 = (float)vx[0];
+  t.A1 = (float)vx[1];
+  t.m1b = g.tric ? (float)vx[2] : 0.0f;
+  t.m1c = g.tric ? (float)vx[3] : 0.0f;
   t.my = sm;
   t.mz = sm + g.ny;
   t.Ay = sm + nyz;
@@ -554,7 +597,8 @@ __device__ __forceinline__ void y_tile(const SysDesc& d, int mode, int tile, flo
 }
 
 // z pass: tx_z consecutive y at one kx, all z (element row of the tile = tx contiguous complex).
-// mode: 0 forward, 1 inverse, 2 forward + solve + inverse, 3 solve only.
+// mode: 0 forward, 1 inverse, 2 forward + solve + inverse, 3 solve only (the staged scalar_sum,
+// with the influence tables computed by the tile itself: no table phase before it).
 // smem: twiddles, two tile buffers, 32*7 int64.
 __device__ __forceinline__ void z_tile(const SysDesc& d, int mode, int tile, float2* smem) {
   const Geom& g = d.g;
@@ -572,11 +616,13 @@ __device__ __forceinline__ void z_tile(const SysDesc& d, int mode, int tile, flo
   const FastDiv txd = make_fastdiv(tx);
   float2* __restrict__ base = d.cgrid + cidx(g, kx, 0, y0);
   const size_t es = (size_t)g.ny;
-  if (mode != 3)
+  const bool solve = mode >= 2;
+  if (mode < 3)
     for (int i = tid; i < L; i += kThreads) tw[i] = __ldg(&d.tw[plan.tw_off + i]);
   // the solve's influence tables load together with the columns (their own smem region)
   KTab kt;
-  if (mode == 2 || mode == 3) kt = stage_ktab(d, kx, ksm);
+  if (mode == 3) kt = stage_ktab_local(d, kx, ksm);
+  else if (mode == 2) kt = stage_ktab(d, kx, ksm);
   for (int idx = tid; idx < L * tx; idx += kThreads) {
     const int e = fdiv(idx, txd), t = idx - e * tx;
     b0[e * ld + t] = t < nt ? __ldcg(&base[e * es + t]) : make_float2(0.0f, 0.0f);
@@ -586,7 +632,7 @@ __device__ __forceinline__ void z_tile(const SysDesc& d, int mode, int tile, flo
   float2* res = b0;
   if (mode == 0 || mode == 2) res = fft_tile(b0, b1, plan, ld, 1, ln, tw, false);
   if (mode == 1) res = fft_tile(b0, b1, plan, ld, 1, ln, tw, true);
-  if (mode == 2 || mode == 3) {
+  if (solve) {
     if (g.tric) {
       solve_span_tric(d, res, ld, L * tx, tx, txd, nt, kx, y0, kt, red);
     } else {
