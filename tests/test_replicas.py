@@ -108,3 +108,35 @@ def test_bench_rank_summary_gloo_two_ranks():
     for _, total_ms, value in res:
         assert total_ms == 20.0 and abs(value - 200 / 0.020) < 1e-6
 
+
+
+def test_bench_fft_schedule_pins_without_autotuning():
+    """`--fft-schedule` (for profilers that cannot launch the cluster build) pins the y/z
+    schedule on every handle the bench makes and skips the autotuner; `auto` autotunes."""
+    import bench
+
+    class FakeHandle:
+        def __init__(self):
+            self.calls = []
+
+        def set_fft_schedule(self, s):
+            self.calls.append(("schedule", s))
+
+        def autotune(self, *a, **k):
+            self.calls.append(("autotune",))
+            return {"schedule": 0}
+
+        def get_tune_config(self):
+            return {"schedule": 0, "x_lines": 16, "y_lines": 16, "z_columns": 16, "grid_ctas": 0}
+
+    class Args:
+        fft_schedule = "passes"
+
+    h = FakeHandle()
+    tune = bench.tune_single(h, Args(), [1.0] * 3, None, 0, 0.3, 3)
+    assert ("autotune",) not in h.calls and tune["schedule"] == bench.SCHEDULES["passes"] and tune["pinned"]
+    Args.fft_schedule = "auto"
+    h = FakeHandle()
+    assert bench.tune_single(h, Args(), [1.0] * 3, None, 0, 0.3, 3) == {"schedule": 0}
+    assert h.calls == [("autotune",)]
+    assert set(bench.SCHEDULES) == {"auto", "planes", "passes", "cluster"}
