@@ -70,3 +70,24 @@ def test_create_validates_before_gpu(lib, args, status):
 def test_null_handle_rejected(lib):
     assert lib.pme_r2c_fft(None) == _capi.PME_EINVAL
     assert lib.pme_destroy(None) == _capi.PME_OK
+
+
+def test_trace_buffer_sizing_host_logic():
+    """The trace hook's buffer check (no GPU needed): 14 entries per CTA plus the 32 step stamps
+    of a single-system trace must fit, and only an int64 CUDA buffer is accepted."""
+    import torch
+    from gpu_recip_b200.pme import TRACE_STEP_STAMPS, _trace_ctas
+
+    class Buf:
+        def __init__(self, n, dtype=torch.int64, cuda=True):
+            self.n, self.dtype, self.is_cuda = n, dtype, cuda
+
+        def numel(self):
+            return self.n
+
+    assert _trace_ctas(Buf(100 * 14 + TRACE_STEP_STAMPS), 0, TRACE_STEP_STAMPS) == 100
+    assert _trace_ctas(Buf(100 * 14), 0, 0) == 100
+    assert _trace_ctas(Buf(100 * 14 + TRACE_STEP_STAMPS), 64, TRACE_STEP_STAMPS) == 64
+    for bad in (Buf(100 * 14), Buf(13), Buf(100 * 14 + 40, torch.int32), Buf(100 * 14 + 40, cuda=False)):
+        with pytest.raises(ValueError):
+            _trace_ctas(bad, 100, TRACE_STEP_STAMPS)
